@@ -1,0 +1,139 @@
+"""ctypes binding of the C-ABI declared in include/tslb.h (libtslb.so).
+
+This is the Python side of the same boundary a Fortran host binds with
+iso_c_binding; every function maps 1:1 onto an `extern "C"` entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtslb.so")
+
+# ---- constants mirrored from include/tslb.h ----
+OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(7)
+MODE_PHASEFIELD, MODE_COLOUR = 0, 1
+PREC_FP32, PREC_BF16, PREC_FP16S = 0, 1, 2
+BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET = range(5)
+FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
+NREDUCE = 12
+RED_NAMES = ("mass", "mass_a", "mass_b", "mom_x", "mom_y", "mom_z", "kinetic",
+             "umax", "rho_in", "rho_out", "dp", "n_in")
+FIELDS = ("rho", "u", "v", "w", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "phi")
+
+
+class TslbParams(ctypes.Structure):
+    """Mirror of `tslb_params` (include/tslb.h)."""
+
+    _fields_ = [
+        ("mode", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("tau_a", ctypes.c_float),
+        ("tau_b", ctypes.c_float),
+        ("sigma", ctypes.c_float),
+        ("beta", ctypes.c_float),
+        ("sharp_c", ctypes.c_float),
+        ("grad_threshold", ctypes.c_float),
+        ("force", ctypes.c_float * 3),
+        ("bc", ctypes.c_int32 * 6),
+        ("bc_u", (ctypes.c_float * 3) * 6),
+        ("bc_phi", ctypes.c_float * 6),
+        ("wall_phi_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+def default_params() -> TslbParams:
+    """Python restatement of tslb_default_params (no library needed)."""
+    p = TslbParams()
+    p.mode = MODE_PHASEFIELD
+    p.precision = PREC_FP32
+    p.tau_a = 0.5004
+    p.tau_b = 0.5004
+    p.sigma = 0.001
+    p.beta = 0.7
+    p.sharp_c = 0.3 * 3
+    p.grad_threshold = 1e-3
+    for f in range(6):
+        p.bc[f] = BC_PERIODIC
+        p.bc_phi[f] = 0.0
+    p.wall_phi_mode = 0
+    return p
+
+
+def make_params(**kw) -> TslbParams:
+    """default_params() with fields overridden by keyword (force/bc/bc_u/bc_phi as sequences)."""
+    p = default_params()
+    for k, v in kw.items():
+        if k == "force":
+            for a in range(3):
+                p.force[a] = float(v[a])
+        elif k == "bc":
+            for f in range(6):
+                p.bc[f] = int(v[f])
+        elif k == "bc_u":
+            for f in range(6):
+                for a in range(3):
+                    p.bc_u[f][a] = float(v[f][a])
+        elif k == "bc_phi":
+            for f in range(6):
+                p.bc_phi[f] = float(v[f])
+        else:
+            setattr(p, k, v)
+    return p
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libtslb.so (built in-tree by entropicthreadsafe_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with entropicthreadsafe_b200.build.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.tslb_default_params.argtypes = [vp]
+        L.tslb_default_params.restype = None
+        L.tslb_create.argtypes = [vp, ip, ip, ip, ctypes.POINTER(vp)]
+        L.tslb_create.restype = ip
+        L.tslb_destroy.argtypes = [vp]
+        L.tslb_destroy.restype = None
+        L.tslb_upload_moments.argtypes = [vp] + [fp] * 11
+        L.tslb_upload_moments.restype = ip
+        L.tslb_upload_pops.argtypes = [vp, fp, fp]
+        L.tslb_upload_pops.restype = ip
+        L.tslb_step.argtypes = [vp, ip]
+        L.tslb_step.restype = ip
+        L.tslb_download_moments.argtypes = [vp] + [fp] * 11
+        L.tslb_download_moments.restype = ip
+        L.tslb_download_normals.argtypes = [vp, fp, fp, fp]
+        L.tslb_download_normals.restype = ip
+        L.tslb_reduce.argtypes = [vp, dp]
+        L.tslb_reduce.restype = ip
+        L.tslb_set_inlet.argtypes = [vp, ip, fp]
+        L.tslb_set_inlet.restype = ip
+        L.tslb_synchronize.argtypes = [vp]
+        L.tslb_synchronize.restype = ip
+        L.tslb_stream.argtypes = [vp]
+        L.tslb_stream.restype = vp
+        L.tslb_launch_count.argtypes = [vp]
+        L.tslb_launch_count.restype = ctypes.c_longlong
+        L.tslb_last_error.argtypes = [vp]
+        L.tslb_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))

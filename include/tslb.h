@@ -1,0 +1,185 @@
+/*
+ * tslb.h -- C-ABI of the B200 thread-safe lattice Boltzmann (TSLB) step.
+ *
+ * One call advances the two-component, recursive-regularized D3Q27 TSLB
+ * step by n time steps on one GPU.  The state lives on the device as 11
+ * moment fields per node (rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi),
+ * where p** is the non-equilibrium second moment Pi^neq.  Host arrays
+ * passed to the upload/download calls are Fortran column-major with x
+ * fastest: element (i,j,k) of an nx*ny*nz field sits at
+ * (i-1) + nx*((j-1) + ny*(k-1)) for 1-based i,j,k, exactly the layout of
+ * the reference's vars-module arrays rho(1:nx,1:ny,1:nz) etc.
+ *
+ * Every entry point returns an int status (TSLB_OK = 0) and never aborts
+ * the process; tslb_last_error() gives the message of the last failure.
+ * Host pointers are borrowed for the duration of the call only.
+ *
+ * Which reference interface each entry point replaces (paths relative to
+ * the reference repository):
+ *   tslb_create          allocate(...) + parameter block of
+ *                        recursive_2c_TSLB3D.f90:20-77 and the
+ *                        "!$acc data copy" region at :316-317
+ *   tslb_upload_pops     the device copy-in of f, g after the initial
+ *                        conditions (recursive_2c_TSLB3D.f90:106-287,316)
+ *                        followed by the moments pass (:346-542)
+ *   tslb_upload_moments  the same copy-in for a moment-space state
+ *                        (TSLB_2C-mpi/lb_kernels_module.f90:938-1142 builds
+ *                        the state from rho, u, Pi)
+ *   tslb_step            one loop iteration of recursive_2c_TSLB3D.f90:344-839:
+ *                        moments (:346-542) + normals (:543-577) +
+ *                        collision and streaming (:607-836) + boundary
+ *                        conditions (:838 -> boundary_cds_3D_module.f90);
+ *                        module form lb_kernels_module.f90:213,738; the
+ *                        colour-gradient operator of
+ *                        turbulent_benchmark/couette/recursive_colorTSLB3D.f90:468-1108
+ *   tslb_download_moments "!$acc update host(rho,phi,u,v,w)"
+ *                        (recursive_2c_TSLB3D.f90:597) before print_module writers
+ *   tslb_download_normals "!$acc update host" of normx/normy/normz
+ *   tslb_set_inlet       the inlet-plane refresh of bcs_2c_turbulent_jet
+ *                        (boundary_cds_3D_module.f90:866-877)
+ *   tslb_reduce          the diagnostics the drivers compute on the host
+ *                        (mass, momentum) and the Laplace pressure check
+ *   tslb_destroy         "!$acc end data" + deallocate (:841)
+ */
+#ifndef TSLB_H
+#define TSLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TSLB_OK               0
+#define TSLB_ERR_ARG          1  /* bad argument (null pointer, size, parameter) */
+#define TSLB_ERR_CUDA         2  /* a CUDA runtime call failed                   */
+#define TSLB_ERR_NAN          3  /* the step produced a non-finite moment        */
+#define TSLB_ERR_TIMEOUT      4  /* a bounded device wait ran out                */
+#define TSLB_ERR_UNSUPPORTED  5  /* valid request this build does not implement  */
+#define TSLB_ERR_STATE        6  /* call out of order (e.g. step before upload)  */
+
+/* ---- two-component operator ---- */
+#define TSLB_MODE_PHASEFIELD  0  /* D3Q7 conservative phase field + CSF velocity shift
+                                    (recursive_2c_TSLB3D.f90); phi in [0,1]          */
+#define TSLB_MODE_COLOUR      1  /* colour gradient: perturbation + recolouring
+                                    (recursive_colorTSLB3D.f90); phi in [-1,1]       */
+
+/* ---- storage precision of the device moment state ---- */
+#define TSLB_PREC_FP32        0
+#define TSLB_PREC_BF16        1  /* shifted moments in bf16, collision in fp32       */
+#define TSLB_PREC_FP16S       2  /* shifted moments in fp16 with per-field 2^k scale */
+
+/* ---- face boundary kinds; faces are ordered x-, x+, y-, y+, z-, z+ ---- */
+#define TSLB_BC_PERIODIC      0  /* wrap (mpi_module.f90:2083-2118 exchange_pops_intpbc) */
+#define TSLB_BC_BOUNCEBACK    1  /* half-way bounce-back (boundary_cds_3D_module.f90:10-76) */
+#define TSLB_BC_VELOCITY      2  /* regularized wall of velocity bc_u
+                                    (bcs_couette_w_regularized..., :405-629)              */
+#define TSLB_BC_INLET         3  /* regularized inlet, per-node velocity and colour plane
+                                    (bcs_2c_turbulent_jet inlet, :931-988)                */
+#define TSLB_BC_OUTLET        4  /* regularized zero-gradient outlet (:990-1048)          */
+
+#define TSLB_NREDUCE         12
+
+/* indices into the tslb_reduce output (all FP64, summed on the device) */
+#define TSLB_RED_MASS         0  /* sum rho                                         */
+#define TSLB_RED_MASS_A       1  /* colour: sum rho(1+phi)/2; phase field: sum phi  */
+#define TSLB_RED_MASS_B       2  /* colour: sum rho(1-phi)/2; phase field: sum 1-phi*/
+#define TSLB_RED_MOM_X        3  /* sum rho u                                       */
+#define TSLB_RED_MOM_Y        4
+#define TSLB_RED_MOM_Z        5
+#define TSLB_RED_KINETIC      6  /* sum rho |u|^2 / 2                               */
+#define TSLB_RED_UMAX         7  /* max |u|                                         */
+#define TSLB_RED_RHO_IN       8  /* mean rho where phi > 0.9                        */
+#define TSLB_RED_RHO_OUT      9  /* mean rho where phi < 0.1 (PF) / < -0.9 (colour)  */
+#define TSLB_RED_DP          10  /* Laplace jump cs^2 (rho_in - rho_out)            */
+#define TSLB_RED_N_IN        11  /* number of nodes with phi > 0.9                  */
+
+typedef struct tslb_params {
+    int32_t mode;           /* TSLB_MODE_*                                          */
+    int32_t precision;      /* TSLB_PREC_*                                          */
+    float   tau_a;          /* relaxation time of component A (phase field: both)   */
+    float   tau_b;          /* relaxation time of component B (colour mode)         */
+    float   sigma;          /* surface tension                                      */
+    float   beta;           /* recolouring parameter (colour mode)                  */
+    float   sharp_c;        /* interface sharpening coefficient (phase field)       */
+    float   grad_threshold; /* colour mode: |grad phi| below which neither the
+                               perturbation nor the recolouring is applied          */
+    float   force[3];       /* constant body force                                  */
+    int32_t bc[6];          /* TSLB_BC_* per face x-, x+, y-, y+, z-, z+            */
+    float   bc_u[6][3];     /* wall / inlet velocity per face (TSLB_BC_VELOCITY);
+                               outlet: x,y used, z replaced by the fluid value;
+                               phase-field outlet: z is the advection speed of g    */
+    float   bc_phi[6];      /* colour carried by incoming populations at velocity
+                               faces (<-2: use the fluid node's own phi) and the
+                               ghost phi of solid faces when wall_phi_mode == 0     */
+    int32_t wall_phi_mode;  /* ghost phi on solid faces: 0 = bc_phi, 1 = mirror     */
+    int32_t reserved[7];
+} tslb_params;
+
+typedef struct tslb_ctx tslb_ctx;
+
+/* Fill *p with the defaults of the reference's two-component program
+ * (recursive_2c_TSLB3D.f90:20-28,45-48): phase field, tau 0.5004,
+ * sigma 0.001, sharp_c 0.9, periodic faces, FP32 storage. */
+void tslb_default_params(tslb_params* p);
+
+/* Validate *p and the sizes, allocate the device state of nx*ny*nz nodes
+ * and a CUDA stream on the current device.  *out is NULL on failure. */
+int  tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out);
+void tslb_destroy(tslb_ctx* ctx);
+
+/* Upload the 11 moment fields (host, Fortran layout, nx*ny*nz floats each).
+ * Pi arguments are the non-equilibrium second moments. */
+int  tslb_upload_moments(tslb_ctx* ctx,
+                         const float* rho, const float* u, const float* v, const float* w,
+                         const float* pxx, const float* pxy, const float* pxz,
+                         const float* pyy, const float* pyz, const float* pzz,
+                         const float* phi);
+
+/* Upload populations in the reference's halo layout f(0:nx+1,0:ny+1,0:nz+1,0:26)
+ * and g(...,0:6) (phase field) or g(...,0:26) (colour: f = component A,
+ * g = component B) and run the moments pass on the device. */
+int  tslb_upload_pops(tslb_ctx* ctx, const float* f, const float* g);
+
+/* Advance nsteps time steps (asynchronous on the context stream). */
+int  tslb_step(tslb_ctx* ctx, int nsteps);
+
+/* Download the moment fields (synchronises).  Any pointer may be NULL. */
+int  tslb_download_moments(tslb_ctx* ctx,
+                           float* rho, float* u, float* v, float* w,
+                           float* pxx, float* pxy, float* pxz,
+                           float* pyy, float* pyz, float* pzz,
+                           float* phi);
+
+/* Download the interface normals n = grad(phi)/(|grad(phi)|+1e-9) of the
+ * current state (recursive_2c_TSLB3D.f90:555-571). */
+int  tslb_download_normals(tslb_ctx* ctx, float* nx, float* ny, float* nz);
+
+/* FP64 diagnostics of the current state, see TSLB_RED_* (synchronises). */
+int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
+
+/* Set the inlet plane of face (TSLB_BC_INLET faces only): uvw_phi holds
+ * four planes (u, v, w, phi) of the face's extent, Fortran order. */
+int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
+
+/* Wait for all work queued on the context stream. */
+int  tslb_synchronize(tslb_ctx* ctx);
+
+/* The context's cudaStream_t, for callers that order their own work or
+ * CUDA events against the step. */
+void* tslb_stream(tslb_ctx* ctx);
+
+/* Number of kernel launches the context has issued since creation. */
+long long tslb_launch_count(tslb_ctx* ctx);
+
+/* Message of the last failed call on ctx (or of the last failed
+ * tslb_create when ctx is NULL).  Never NULL. */
+const char* tslb_last_error(tslb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSLB_H */

@@ -1,0 +1,77 @@
+"""The CPU oracle against golden vectors of the reference's own statements.
+
+tests/golden/*.npz hold populations and moments produced by evaluating the
+reference's Fortran statements with numpy (tests/golden/make_golden.py):
+the phase-field step recursive_2c_TSLB3D.f90:351-832, the forced collision
+TSLB_2C-mpi/lb_kernels_module.f90:747-931, bounce-back
+boundary_cds_3D_module.f90:18-70 and the moving-wall condition
+boundary_cds_3D_module.f90:413-571.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from entropicthreadsafe_b200 import capi
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = ("pf_periodic", "pf_walls_force", "couette")
+
+
+def golden_params(meta):
+    bc = [capi.BC_PERIODIC] * 6
+    bcu = [[0.0, 0.0, 0.0]] * 6
+    if meta["walls"] == "bounceback":
+        bc[4] = bc[5] = capi.BC_BOUNCEBACK
+    elif meta["walls"] == "couette":
+        bc[4] = bc[5] = capi.BC_VELOCITY
+        bcu = [[0, 0, 0]] * 4 + [[-meta["uwall"], 0, 0], [meta["uwall"], 0, 0]]
+    return capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=meta["tau"], sigma=meta["sigma"],
+                            sharp_c=meta["sharp_c"], force=meta["force"], bc=bc, bc_u=bcu,
+                            bc_phi=[0.0] * 6, wall_phi_mode=0)
+
+
+def load(case):
+    d = np.load(os.path.join(GOLDEN, case + ".npz"))
+    return d, json.loads(str(d["meta"]))
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_fp64_matches_reference_statements(case):
+    d, meta = load(case)
+    nz, ny, nx = d["rho_fp64"].shape
+    o = oracle.Oracle(golden_params(meta), nx, ny, nz, fp64=True)
+    o.set_pops(d["f_fp64"], d["g_fp64"])
+    o.step(meta["nsteps"])
+    out = o.get_moments()
+    for m in capi.FIELDS:
+        # double-precision round-off only: the two forms of the polynomials differ
+        assert rel_err(out[m], d[m + "_fp64"]) < 1e-12, m
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_fp32_matches_reference_statements(case):
+    d, meta = load(case)
+    nz, ny, nx = d["rho_fp32"].shape
+    o = oracle.Oracle(golden_params(meta), nx, ny, nz, fp64=False)
+    o.set_pops(d["f_fp32"], d["g_fp32"])
+    o.step(meta["nsteps"])
+    out = o.get_moments()
+    # FP32 round-off of two algebraically equal forms, relative to each field's max
+    tol = {"rho": 2e-6, "u": 2e-5, "v": 2e-5, "w": 5e-5, "phi": 2e-6}
+    for m in capi.FIELDS:
+        assert rel_err(out[m], d[m + "_fp32"]) < tol.get(m, 2e-4), m
+
+
+def test_reference_fp32_noise_is_what_the_gpu_tolerance_assumes():
+    # the reference's own FP32 statements against its FP64 statements: the
+    # noise floor that any FP32 implementation of this step shares
+    d, _ = load("pf_periodic")
+    for m in capi.FIELDS:
+        assert rel_err(d[m + "_fp32"], d[m + "_fp64"]) < 2e-4, m
