@@ -1,0 +1,324 @@
+"""Benchmark of the two-component D3Q27 TSLB step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one time step of the fused CUDA kernel over the whole
+lattice.  The workload is the two-component colour-gradient channel
+384x192x128 (x, y periodic, half-way bounce-back walls at z, body force
+gx = 2.5e-6, nu = 0.0015, 40 droplets of radius 8), FP32 state resident in
+HBM.  The state (830 MB) is larger than the 126 MB L2, so no flush is
+needed between steps.
+
+Under torchrun every rank advances its own independent copy of the channel
+on its own GPU (replicas, weak scaling): the step has no inter-GPU
+exchange on one domain, so there is no collective on the data path.
+Timing: CUDA events on the library's stream around exactly K steps,
+bracketed by a barrier and a device synchronize, max over ranks.
+
+--impl reference times the CPU path of the reference algorithm on the
+host cores: the C++ restatement under oracle/ (the reference is Fortran
+and no Fortran compiler exists on these machines), all host threads, on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES_PER_NODE = 88  # 11 FP32 moments read + 11 written per lattice update
+METRIC = "MLUPS"
+UNIT = "MLUPS"
+WORKLOAD = ("channel 384x192x128 two-component colour-gradient recursive-regularized D3Q27 TSLB, "
+            "x/y periodic, z half-way bounce-back, gx=2.5e-6, nu=0.0015, 40 droplets R=8, sigma=0.005, beta=0.7")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_node():
+    """DRAM bytes per lattice update of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["dram_bytes_per_node"]), d
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        def rd():
+            for line in self.proc.stdout:
+                self.lines.append(line.strip())
+        self.thread = threading.Thread(target=rd, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(max_seconds: float = 20.0):
+    """Time the oracle (C++ restatement of the reference CPU path, OpenMP, FP32)
+    on the channel workload: full size if a step fits the budget, else z-slab samples."""
+    import oracle
+    from entropicthreadsafe_b200 import workloads
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    nz = 128
+    while True:
+        p, f = workloads.channel(nz=nz) if nz == 128 else workloads.channel(nz=nz, ndrops=max(1, 40 * nz // 128))
+        ny, nx = f["rho"].shape[1], f["rho"].shape[2]
+        o = oracle.Oracle(p, nx, ny, nz, fp64=False, fast=True)
+        o.set_moments({k: v.astype(np.float64) for k, v in f.items()})
+        t0 = time.perf_counter()
+        o.step(1)
+        t1 = time.perf_counter() - t0
+        if t1 * 3 <= max_seconds or nz <= 8:
+            break
+        o.close()
+        nz = max(8, nz // 2)
+    steps = max(1, int(max_seconds / max(t1, 1e-6)) - 1)
+    steps = min(steps, 50)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    nodes = nx * ny * nz
+    return {"value": nodes * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle (C++ restatement of the reference CPU path, FP32, OpenMP) on the channel "
+                      f"{nx}x{ny}x{nz}, {steps} steps after 1 warm-up step, {dt:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    base = cpu_baseline(max_seconds=max(5.0, min(60.0, 3.0 * (args.steps + args.warmup))))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded channel initial state)",
+        "config": {"workload": WORKLOAD, "nx": 384, "ny": 192, "nz": 128},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def e2e_run(args, p, f, ws):
+    """The same metric through the public API with host buffers: create,
+    upload from pinned host memory, K x (step + FP64 diagnostics read back),
+    download to pinned host memory; wall clock, max over ranks."""
+    import torch
+    from entropicthreadsafe_b200 import capi
+    from entropicthreadsafe_b200.solver import Lattice
+    nz, ny, nx = f["rho"].shape
+    nodes = nx * ny * nz
+    pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float32, pin_memory=True) for k in capi.FIELDS}
+    for k in capi.FIELDS:
+        pinned[k].numpy()[...] = f[k]
+    host_in = {k: pinned[k].numpy() for k in capi.FIELDS}
+    out_pinned = {k: torch.empty((nz, ny, nx), dtype=torch.float32, pin_memory=True) for k in capi.FIELDS}
+    host_out = {k: out_pinned[k].numpy() for k in capi.FIELDS}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lat2 = Lattice(p, nx, ny, nz)
+    lat2.upload_moments(host_in)
+    for _ in range(args.steps):
+        lat2.step(1)
+        lat2.reduce()
+    lat2.download(host_out)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    lat2.close()
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = 11 * 4 * nodes
+    return {"value": ws * nodes * args.steps / e2e_s / 1e6, "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes / args.steps,
+            "d2h_bytes_per_step": state_bytes / args.steps + 8 * capi.NREDUCE,
+            "what": "tslb_create + tslb_upload_moments (pinned host) + K x (tslb_step(1) + tslb_reduce) "
+                    "+ tslb_download_moments, wall clock, per step"}
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    from entropicthreadsafe_b200 import capi, workloads
+    from entropicthreadsafe_b200.solver import Lattice
+
+    p, f = workloads.channel(nz=args.nz) if args.nz else workloads.channel()
+    nz, ny, nx = f["rho"].shape
+    nodes = nx * ny * nz
+
+    def barrier_sync():
+        torch.cuda.synchronize()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    lat = Lattice(p, nx, ny, nz)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    lat.upload_moments(f)
+    lat.step(args.warmup)
+    lat.synchronize()
+    # ---- device-resident timing ----
+    barrier_sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = lat.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    lat.step(args.steps)
+    ev1.record(stream)
+    lat.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = lat.launches - l0
+    clk = clocks.stop()
+    barrier_sync()
+    red = lat.reduce()
+    ms_max = ms
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ws * nodes * args.steps / (ms_max * 1e-3) / 1e6
+    ms_step = ms_max / args.steps
+    # ---- end to end through the public API with host buffers ----
+    lat.close()
+    barrier_sync()
+    e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
+    state_bytes = 11 * 4 * nodes
+    # ---- roofline of the step kernel ----
+    peak, peak_kind = peaks()
+    alg_bytes = ALG_BYTES_PER_NODE * nodes
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    tpn, tinfo = traffic_per_node()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tpn * nodes if tpn else None, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": alg_bytes, "kernel": "tslb::step_kernel<colour>"}
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+    base = cpu_baseline(max_seconds=20.0) if ws == 1 and not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded channel initial state, counter-based noise)",
+        "config": {"workload": WORKLOAD, "nx": nx, "ny": ny, "nz": nz, "nodes_per_gpu": nodes,
+                   "parallelism": f"replicas x{ws}", "l2": "state 830 MB > 126 MB L2, no flush needed",
+                   "state_bytes": state_bytes},
+        "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk, "check": {"mass": red["mass"], "umax": red["umax"], "mass_a": red["mass_a"]},
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--nz", type=int, default=0, help="shallower channel (profiling runs only)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

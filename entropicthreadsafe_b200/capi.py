@@ -55,7 +55,7 @@ def default_params() -> TslbParams:
     p.tau_b = 0.5004
     p.sigma = 0.001
     p.beta = 0.7
-    p.sharp_c = 0.3 * 3
+    p.sharp_c = float(np.float32(0.3) * np.float32(3))  # single-precision 0.3*3 of the reference
     p.grad_threshold = 1e-3
     for f in range(6):
         p.bc[f] = BC_PERIODIC

@@ -1,0 +1,497 @@
+// tslb.cu -- C-ABI (include/tslb.h) of the B200 TSLB step: context,
+// device state, uploads/downloads, the step launch and FP64 diagnostics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tslb.h"
+#include "tslb_step.cuh"
+
+using namespace tslb;
+
+struct tslb_ctx {
+    tslb_params p;
+    int nx, ny, nz;
+    long long n;        // nodes
+    long long N;        // padded field stride
+    int device;
+    cudaStream_t stream = nullptr;
+    float* state[2] = {nullptr, nullptr};  // ping-pong, 11 fields each
+    int cur = 0;
+    float* nrm = nullptr;                  // 3 fields
+    float* inlet[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    unsigned int* flags = nullptr;
+    double* red = nullptr;                 // reduction accumulators
+    bool loaded = false;
+    int zchunk = 32;
+    long long launches = 0;
+    std::string err;
+};
+
+static std::string g_create_error;
+
+namespace {
+
+int fail(tslb_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(ctx, TSLB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+long long face_area(const tslb_ctx* c, int face) {
+    int ax = face / 2;
+    return ax == 0 ? (long long)c->ny * c->nz : ax == 1 ? (long long)c->nx * c->nz : (long long)c->nx * c->ny;
+}
+
+int validate(const tslb_params* p, int nx, int ny, int nz, std::string& why) {
+    if (!p) { why = "params is NULL"; return TSLB_ERR_ARG; }
+    if (nx < 1 || ny < 1 || nz < 1) { why = "sizes must be >= 1"; return TSLB_ERR_ARG; }
+    if ((long long)nx * ny * nz > (1LL << 36)) { why = "lattice too large"; return TSLB_ERR_ARG; }
+    if (p->mode != TSLB_MODE_PHASEFIELD && p->mode != TSLB_MODE_COLOUR) { why = "unknown mode"; return TSLB_ERR_ARG; }
+    if (p->precision != TSLB_PREC_FP32) { why = "only TSLB_PREC_FP32 storage is implemented"; return TSLB_ERR_UNSUPPORTED; }
+    if (!(p->tau_a > 0.5f) || !std::isfinite(p->tau_a)) { why = "tau_a must be > 0.5"; return TSLB_ERR_ARG; }
+    if (p->mode == TSLB_MODE_COLOUR && (!(p->tau_b > 0.5f) || !std::isfinite(p->tau_b))) { why = "tau_b must be > 0.5"; return TSLB_ERR_ARG; }
+    if (!std::isfinite(p->sigma) || !std::isfinite(p->beta) || !std::isfinite(p->sharp_c) || !std::isfinite(p->grad_threshold)) {
+        why = "non-finite parameter"; return TSLB_ERR_ARG;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(p->force[a])) { why = "non-finite force"; return TSLB_ERR_ARG; }
+    for (int f = 0; f < 6; ++f) {
+        if (p->bc[f] < TSLB_BC_PERIODIC || p->bc[f] > TSLB_BC_OUTLET) { why = "unknown boundary kind"; return TSLB_ERR_ARG; }
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(p->bc_u[f][a])) { why = "non-finite wall velocity"; return TSLB_ERR_ARG; }
+    }
+    for (int ax = 0; ax < 3; ++ax) {
+        bool pm = p->bc[2 * ax] == TSLB_BC_PERIODIC, pp = p->bc[2 * ax + 1] == TSLB_BC_PERIODIC;
+        if (pm != pp) { why = "periodic faces must come in pairs"; return TSLB_ERR_ARG; }
+    }
+    if (p->wall_phi_mode != 0 && p->wall_phi_mode != 1) { why = "wall_phi_mode must be 0 or 1"; return TSLB_ERR_ARG; }
+    return TSLB_OK;
+}
+
+StepArgs make_args(tslb_ctx* c, const float* in, float* out) {
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = c->N;
+    a.in = in; a.out = out; a.nrm = c->nrm;
+    a.zchunk = c->zchunk;
+    a.mode = c->p.mode;
+    a.omega_pf = 1.0f / c->p.tau_a;
+    a.inv_nu_a = 3.0f / (c->p.tau_a - 0.5f);
+    a.inv_nu_b = 3.0f / ((c->p.mode == TSLB_MODE_COLOUR ? c->p.tau_b : c->p.tau_a) - 0.5f);
+    a.sigma = c->p.sigma; a.beta = c->p.beta; a.sharp = c->p.sharp_c; a.thr = c->p.grad_threshold;
+    a.acoef = 4.5f;  // A = 9/2 sigma omega gives the Laplace jump 2 sigma / R for phi in [-1, 1]
+    for (int k = 0; k < 3; ++k) a.force[k] = c->p.force[k];
+    a.wall_phi_mode = c->p.wall_phi_mode;
+    for (int f = 0; f < 6; ++f) {
+        a.face[f].kind = c->p.bc[f];
+        for (int k = 0; k < 3; ++k) a.face[f].u[k] = c->p.bc_u[f][k];
+        a.face[f].phi = c->p.bc_phi[f];
+        a.face[f].plane = c->inlet[f];
+    }
+    a.flags = c->flags;
+    return a;
+}
+
+// ---------------------------------------------------------------- kernels
+__global__ void normals_kernel(const StepArgs a, float* nrm) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    if (i >= n) return;
+    const int x = (int)(i % a.nx), y = (int)((i / a.nx) % a.ny), z = (int)(i / ((long long)a.nx * a.ny));
+    float g[3];
+    grad_phi(a, x, y, z, g);
+    const float den = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + 1e-9f;
+    nrm[i] = g[0] / den;
+    nrm[a.N + i] = g[1] / den;
+    nrm[2 * a.N + i] = g[2] / den;
+}
+
+// rho (host layout) -> rho - 1 in place
+__global__ void shift_rho_kernel(float* d, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) d[i] = d[i] - 1.0f;
+}
+
+// Moments pass of the reference on populations in its halo layout
+// (recursive_2c_TSLB3D.f90:351-539; colour: both sets, recursive_colorTSLB3D.f90:482-671).
+__constant__ int c_cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, -1, 1, 1, -1};
+__constant__ int c_cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, -1, 1, -1, 1};
+__constant__ int c_cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1};
+__constant__ int c_piorder[26] = {1, 2, 3, 4, 5, 6, 7, 8, 10, 9, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26};
+
+__device__ float feq_over_w_dev(int q, float rho, float u, float v, float w) {
+    const float cx = (float)c_cx[q], cy = (float)c_cy[q], cz = (float)c_cz[q];
+    const float t = 1.f / 3.f;
+    const float cu = cx * u + cy * v + cz * w, uu = u * u + v * v + w * w;
+    const float h3 = 13.5f * ((cx * cx - t) * cy * u * u * v + (cx * cx - t) * cz * u * u * w +
+                              (cy * cy - t) * cx * u * v * v + (cy * cy - t) * cz * v * v * w +
+                              (cz * cz - t) * cx * u * w * w + (cz * cz - t) * cy * v * w * w) +
+                     27.f * cx * cy * cz * u * v * w;
+    return rho * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * uu + h3);
+}
+
+__global__ void pops_to_moments_kernel(int nx, int ny, int nz, long long N, int colour,
+                                       const float* __restrict__ f, const float* __restrict__ g, float* out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long n = (long long)nx * ny * nz;
+    if (i >= n) return;
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+    const long long sx = nx + 2, sy = ny + 2, vol = sx * sy * (nz + 2);
+    const long long h = (x + 1) + sx * ((y + 1) + sy * (long long)(z + 1));
+    float tot[27];
+    float ra = 0.f, rb = 0.f, phi = 0.f;
+    for (int q = 0; q < 27; ++q) { tot[q] = f[q * vol + h]; ra += tot[q]; }
+    if (colour) {
+        for (int q = 0; q < 27; ++q) { float gb = g[q * vol + h]; rb += gb; tot[q] += gb; }
+    } else {
+        for (int q = 0; q < 7; ++q) phi += g[q * vol + h];
+    }
+    const float rho = colour ? ra + rb : ra;
+    if (colour) phi = (ra - rb) / rho;
+    float sp[3] = {0.f, 0.f, 0.f}, sm[3] = {0.f, 0.f, 0.f};
+    for (int q = 1; q < 27; ++q) {
+        const int c[3] = {c_cx[q], c_cy[q], c_cz[q]};
+        for (int a = 0; a < 3; ++a) {
+            if (c[a] > 0) sp[a] += tot[q];
+            if (c[a] < 0) sm[a] += tot[q];
+        }
+    }
+    const float u = (sp[0] - sm[0]) / rho, v = (sp[1] - sm[1]) / rho, w = (sp[2] - sm[2]) / rho;
+    float P[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < 26; ++k) {
+        const int q = c_piorder[k];
+        const float wq = wclass(c_cx[q] * c_cx[q] + c_cy[q] * c_cy[q] + c_cz[q] * c_cz[q]);
+        const float fneq = tot[q] - wq * feq_over_w_dev(q, rho, u, v, w);
+        const int cx = c_cx[q], cy = c_cy[q], cz = c_cz[q];
+        if (cx) P[0] += fneq;
+        if (cx * cy > 0) P[1] += fneq; else if (cx * cy < 0) P[1] -= fneq;
+        if (cx * cz > 0) P[2] += fneq; else if (cx * cz < 0) P[2] -= fneq;
+        if (cy) P[3] += fneq;
+        if (cy * cz > 0) P[4] += fneq; else if (cy * cz < 0) P[4] -= fneq;
+        if (cz) P[5] += fneq;
+    }
+    out[F_D * N + i] = rho - 1.0f;
+    out[F_U * N + i] = u; out[F_V * N + i] = v; out[F_W * N + i] = w;
+    out[F_XX * N + i] = P[0]; out[F_XY * N + i] = P[1]; out[F_XZ * N + i] = P[2];
+    out[F_YY * N + i] = P[3]; out[F_YZ * N + i] = P[4]; out[F_ZZ * N + i] = P[5];
+    out[F_PHI * N + i] = phi;
+}
+
+// FP64 diagnostics: sums in TSLB_RED_* order (8..9 hold sums of rho and
+// counts inside/outside; finalised on the host), umax as float bits.
+constexpr int RED_SLOTS = 12;
+__global__ void reduce_kernel(const float* __restrict__ s, long long n, long long N, int colour, double* red) {
+    __shared__ double sh[RED_SLOTS][8];
+    __shared__ float shmax[8];
+    double acc[RED_SLOTS];
+    for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
+    float umax2 = 0.f;
+    const float lo = colour ? -0.9f : 0.1f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double d = s[F_D * N + i], rho = 1.0 + d;
+        const double u = s[F_U * N + i], v = s[F_V * N + i], w = s[F_W * N + i], phi = s[F_PHI * N + i];
+        acc[0] += d;  // mass - n, exact for small deviations
+        if (colour) { acc[1] += rho * (1.0 + phi) * 0.5; acc[2] += rho * (1.0 - phi) * 0.5; }
+        else { acc[1] += phi; acc[2] += 1.0 - phi; }
+        acc[3] += rho * u; acc[4] += rho * v; acc[5] += rho * w;
+        const double uu = u * u + v * v + w * w;
+        acc[6] += 0.5 * rho * uu;
+        umax2 = fmaxf(umax2, (float)uu);
+        if (phi > 0.9) { acc[7] += rho; acc[8] += 1.0; }
+        if (phi < lo) { acc[9] += rho; acc[10] += 1.0; }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < RED_SLOTS; ++k) {
+        double vv = acc[k];
+        for (int o = 16; o > 0; o >>= 1) vv += __shfl_down_sync(0xffffffffu, vv, o);
+        if (lane == 0) sh[k][warp] = vv;
+    }
+    for (int o = 16; o > 0; o >>= 1) umax2 = fmaxf(umax2, __shfl_down_sync(0xffffffffu, umax2, o));
+    if (lane == 0) shmax[warp] = umax2;
+    __syncthreads();
+    if (threadIdx.x < RED_SLOTS) {
+        double t = 0.0;
+        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) t += sh[threadIdx.x][w8];
+        atomicAdd(&red[threadIdx.x], t);
+    }
+    if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) m = fmaxf(m, shmax[w8]);
+        atomicMax(reinterpret_cast<unsigned int*>(&red[RED_SLOTS]), __float_as_uint(m));
+    }
+}
+
+int check_flags(tslb_ctx* c) {
+    unsigned int h = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&h, c->flags, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (h & 1u) {
+        CUDA_TRY(c, cudaMemsetAsync(c->flags, 0, sizeof(unsigned int), c->stream));
+        return fail(c, TSLB_ERR_NAN, "the step produced a non-finite moment");
+    }
+    return TSLB_OK;
+}
+
+int launch_normals(tslb_ctx* c) {
+    StepArgs a = make_args(c, c->state[c->cur], nullptr);
+    const int bs = 256;
+    const long long grid = (c->n + bs - 1) / bs;
+    normals_kernel<<<(unsigned)grid, bs, 0, c->stream>>>(a, c->nrm);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
+size_t step_smem() { return sizeof(float) * 2 * NCOEF * CAREA; }
+
+int launch_step(tslb_ctx* c) {
+    if (c->p.mode == TSLB_MODE_PHASEFIELD) {
+        int rc = launch_normals(c);
+        if (rc) return rc;
+    }
+    StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
+    dim3 block(TX, TY, 1);
+    dim3 grid((c->nx + TX - 1) / TX, (c->ny + TY - 1) / TY, (c->nz + c->zchunk - 1) / c->zchunk);
+    if (c->p.mode == TSLB_MODE_COLOUR)
+        step_kernel<TSLB_MODE_COLOUR><<<grid, block, step_smem(), c->stream>>>(a);
+    else
+        step_kernel<TSLB_MODE_PHASEFIELD><<<grid, block, step_smem(), c->stream>>>(a);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    c->cur ^= 1;
+    return TSLB_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C-ABI
+extern "C" {
+
+void tslb_default_params(tslb_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->mode = TSLB_MODE_PHASEFIELD;
+    p->precision = TSLB_PREC_FP32;
+    p->tau_a = 0.5004f;  // recursive_2c_TSLB3D.f90:21
+    p->tau_b = 0.5004f;
+    p->sigma = 0.001f;   // :27
+    p->beta = 0.7f;
+    p->sharp_c = 0.3f * 3;  // :28
+    p->grad_threshold = 1e-3f;  // recursive_colorTSLB3D.f90:763
+    for (int f = 0; f < 6; ++f) { p->bc[f] = TSLB_BC_PERIODIC; p->bc_phi[f] = 0.f; }
+    p->wall_phi_mode = 0;
+}
+
+int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
+    if (!out) return fail(nullptr, TSLB_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    std::string why;
+    int rc = validate(p, nx, ny, nz, why);
+    if (rc) return fail(nullptr, rc, why);
+    tslb_ctx* c = new (std::nothrow) tslb_ctx();
+    if (!c) return fail(nullptr, TSLB_ERR_ARG, "out of host memory");
+    c->p = *p;
+    c->nx = nx; c->ny = ny; c->nz = nz;
+    c->n = (long long)nx * ny * nz;
+    c->N = (c->n + 31) / 32 * 32;
+    auto bail = [&](cudaError_t e, const char* what) {
+        g_create_error = std::string(what) + ": " + cudaGetErrorString(e);
+        tslb_destroy(c);
+        return TSLB_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaGetDevice(&c->device)) != cudaSuccess) return bail(e, "cudaGetDevice");
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "cudaStreamCreate");
+    for (int b = 0; b < 2; ++b)
+        if ((e = cudaMalloc(&c->state[b], sizeof(float) * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+    if ((e = cudaMalloc(&c->nrm, sizeof(float) * 3 * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(normals)");
+    if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
+    if ((e = cudaMalloc(&c->red, sizeof(double) * (RED_SLOTS + 1))) != cudaSuccess) return bail(e, "cudaMalloc(reduce)");
+    if ((e = cudaMemset(c->flags, 0, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMemset");
+    for (int f = 0; f < 6; ++f) {
+        if (p->bc[f] != TSLB_BC_INLET) continue;
+        size_t bytes = sizeof(float) * 4 * face_area(c, f);
+        if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
+        if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
+    }
+    static const size_t smem = step_smem();
+    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return bail(e, "cudaFuncSetAttribute");
+    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return bail(e, "cudaFuncSetAttribute");
+    // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+    long long want = 8LL * sms;
+    int zc = (int)std::max<long long>(8, (tiles * nz + want - 1) / want);
+    c->zchunk = std::min(zc, nz);
+    *out = c;
+    return TSLB_OK;
+}
+
+void tslb_destroy(tslb_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int b = 0; b < 2; ++b) cudaFree(c->state[b]);
+    cudaFree(c->nrm);
+    cudaFree(c->flags);
+    cudaFree(c->red);
+    for (int f = 0; f < 6; ++f) cudaFree(c->inlet[f]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int tslb_upload_moments(tslb_ctx* c, const float* rho, const float* u, const float* v, const float* w,
+                        const float* pxx, const float* pxy, const float* pxz, const float* pyy,
+                        const float* pyz, const float* pzz, const float* phi) {
+    if (!c) return TSLB_ERR_ARG;
+    const float* src[NF] = {rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi};
+    for (int f = 0; f < NF; ++f)
+        if (!src[f]) return fail(c, TSLB_ERR_ARG, "tslb_upload_moments: NULL field");
+    float* s = c->state[c->cur];
+    for (int f = 0; f < NF; ++f)
+        CUDA_TRY(c, cudaMemcpyAsync(s + f * c->N, src[f], sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+    const int bs = 256;
+    shift_rho_kernel<<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(s + F_D * c->N, c->n);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->loaded = true;
+    return TSLB_OK;
+}
+
+int tslb_upload_pops(tslb_ctx* c, const float* f, const float* g) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!f || !g) return fail(c, TSLB_ERR_ARG, "tslb_upload_pops: NULL populations");
+    const long long vol = (long long)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+    const int nqg = c->p.mode == TSLB_MODE_COLOUR ? 27 : 7;
+    float *df = nullptr, *dg = nullptr;
+    CUDA_TRY(c, cudaMalloc(&df, sizeof(float) * 27 * vol));
+    cudaError_t e = cudaMalloc(&dg, sizeof(float) * nqg * vol);
+    if (e != cudaSuccess) { cudaFree(df); return fail(c, TSLB_ERR_CUDA, std::string("cudaMalloc(g): ") + cudaGetErrorString(e)); }
+    e = cudaMemcpyAsync(df, f, sizeof(float) * 27 * vol, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dg, g, sizeof(float) * nqg * vol, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        const int bs = 128;
+        pops_to_moments_kernel<<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(
+            c->nx, c->ny, c->nz, c->N, c->p.mode == TSLB_MODE_COLOUR, df, dg, c->state[c->cur]);
+        c->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(df);
+    cudaFree(dg);
+    if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string("tslb_upload_pops: ") + cudaGetErrorString(e));
+    c->loaded = true;
+    return TSLB_OK;
+}
+
+int tslb_step(tslb_ctx* c, int nsteps) {
+    if (!c) return TSLB_ERR_ARG;
+    if (nsteps < 0) return fail(c, TSLB_ERR_ARG, "nsteps < 0");
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "tslb_step before an upload");
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = launch_step(c);
+        if (rc) return rc;
+    }
+    return TSLB_OK;
+}
+
+int tslb_download_moments(tslb_ctx* c, float* rho, float* u, float* v, float* w, float* pxx, float* pxy,
+                          float* pxz, float* pyy, float* pyz, float* pzz, float* phi) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "download before an upload");
+    float* dst[NF] = {rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi};
+    const float* s = c->state[c->cur];
+    for (int f = 0; f < NF; ++f)
+        if (dst[f]) CUDA_TRY(c, cudaMemcpyAsync(dst[f], s + f * c->N, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (rho)
+        for (long long i = 0; i < c->n; ++i) rho[i] = 1.0f + rho[i];
+    return check_flags(c);
+}
+
+int tslb_download_normals(tslb_ctx* c, float* nx, float* ny, float* nz) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "download before an upload");
+    int rc = launch_normals(c);
+    if (rc) return rc;
+    float* dst[3] = {nx, ny, nz};
+    for (int k = 0; k < 3; ++k)
+        if (dst[k]) CUDA_TRY(c, cudaMemcpyAsync(dst[k], c->nrm + k * c->N, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return TSLB_OK;
+}
+
+int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
+    if (!c || !out) return fail(c, TSLB_ERR_ARG, "tslb_reduce: NULL");
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "reduce before an upload");
+    CUDA_TRY(c, cudaMemsetAsync(c->red, 0, sizeof(double) * (RED_SLOTS + 1), c->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    reduce_kernel<<<(unsigned)(sms * 4), 256, 0, c->stream>>>(c->state[c->cur], c->n, c->N,
+                                                               c->p.mode == TSLB_MODE_COLOUR, c->red);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    double h[RED_SLOTS + 1];
+    CUDA_TRY(c, cudaMemcpyAsync(h, c->red, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    unsigned int umax_bits;
+    std::memcpy(&umax_bits, &h[RED_SLOTS], sizeof(umax_bits));
+    float umax2;
+    std::memcpy(&umax2, &umax_bits, sizeof(umax2));
+    out[TSLB_RED_MASS] = (double)c->n + h[0];
+    out[TSLB_RED_MASS_A] = h[1];
+    out[TSLB_RED_MASS_B] = h[2];
+    out[TSLB_RED_MOM_X] = h[3];
+    out[TSLB_RED_MOM_Y] = h[4];
+    out[TSLB_RED_MOM_Z] = h[5];
+    out[TSLB_RED_KINETIC] = h[6];
+    out[TSLB_RED_UMAX] = std::sqrt((double)umax2);
+    out[TSLB_RED_RHO_IN] = h[8] > 0 ? h[7] / h[8] : 0.0;
+    out[TSLB_RED_RHO_OUT] = h[10] > 0 ? h[9] / h[10] : 0.0;
+    out[TSLB_RED_DP] = (h[8] > 0 && h[10] > 0) ? (out[TSLB_RED_RHO_IN] - out[TSLB_RED_RHO_OUT]) / 3.0 : 0.0;
+    out[TSLB_RED_N_IN] = h[8];
+    return check_flags(c);
+}
+
+int tslb_set_inlet(tslb_ctx* c, int face, const float* uvw_phi) {
+    if (!c) return TSLB_ERR_ARG;
+    if (face < 0 || face > 5 || !uvw_phi) return fail(c, TSLB_ERR_ARG, "tslb_set_inlet: bad face or NULL plane");
+    if (c->p.bc[face] != TSLB_BC_INLET || !c->inlet[face]) return fail(c, TSLB_ERR_ARG, "tslb_set_inlet: face is not an inlet");
+    CUDA_TRY(c, cudaMemcpyAsync(c->inlet[face], uvw_phi, sizeof(float) * 4 * face_area(c, face), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return TSLB_OK;
+}
+
+int tslb_synchronize(tslb_ctx* c) {
+    if (!c) return TSLB_ERR_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_flags(c);
+}
+
+void* tslb_stream(tslb_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+long long tslb_launch_count(tslb_ctx* c) { return c ? c->launches : 0; }
+
+const char* tslb_last_error(tslb_ctx* c) {
+    if (!c) return g_create_error.c_str();
+    return c->err.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,327 @@
+// tslb_device.cuh -- device-side building blocks of the fused TSLB step.
+//
+// State layout in HBM: 11 SoA fields of nx*ny*nz floats (x fastest, field
+// stride N padded to 32 floats):
+//   0 d = rho - 1   1 u   2 v   3 w   4 pxx 5 pxy 6 pxz 7 pyy 8 pyz 9 pzz  10 phi
+// p** is the non-equilibrium second moment Pi^neq.  Storing rho - 1 keeps
+// the density's small deviations exact to FP32 round-off of the deviation.
+//
+// Post-collision populations are written as f_c = w_c (1 + P'(c)) where
+// P'(c) is a polynomial in the components of c with 17 per-node
+// coefficients (the monomials 1, cx, cy, cz, cx^2, ..., cx cy cz that
+// survive on D3Q27 because c_a^3 = c_a).  The coefficients fold:
+//   f^eq(rho, u_s) in third-order Hermite form
+//     (recursive_2c_TSLB3D.f90:639-804 "feqs")
+//   (1 - omega) w a^neq(Pi, u), the recursive regularized non-equilibrium
+//     (recursive_2c_TSLB3D.f90:640-805 "fneq1")
+//   colour mode: the perturbation operator and the force source of
+//     turbulent_benchmark/couette/recursive_colorTSLB3D.f90:765-959
+// so that every pulled population costs a handful of FMAs.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/tslb.h"
+
+namespace tslb {
+
+constexpr int NF = 11;
+enum { F_D = 0, F_U, F_V, F_W, F_XX, F_XY, F_XZ, F_YY, F_YZ, F_ZZ, F_PHI };
+
+// coefficient slots (per node, shared memory)
+enum {
+    K_0 = 0, K_X, K_Y, K_Z, K_XX, K_YY, K_ZZ, K_XY, K_XZ, K_YZ,
+    K_XXY, K_XXZ, K_XYY, K_YYZ, K_XZZ, K_YZZ, K_XYZ,
+    K_C0, K_C1, K_C2, K_C3, K_C4,   // colour: phi, Bx, By, Bz, delta0 | phase field: G0, G1x, G1y, G1z, -
+    NCOEF
+};
+
+// accumulator slots of a target node
+enum { A_RHO = 0, A_JX, A_JY, A_JZ, A_XX, A_XY, A_XZ, A_YY, A_YZ, A_ZZ, A_COL, NACC };
+
+constexpr int TX = 32;  // block tile in x (one warp row)
+constexpr int TY = 8;   // block tile in y
+constexpr int CW = TX + 2, CH = TY + 2, CAREA = CW * CH;
+
+// lattice weights by |c|^2 (recursive_2c_TSLB3D.f90:71-74)
+__host__ __device__ constexpr float wclass(int c2) {
+    return c2 == 0 ? 8.0f / 27.0f : c2 == 1 ? 2.0f / 27.0f : c2 == 2 ? 1.0f / 54.0f : 1.0f / 216.0f;
+}
+// 1/|c| by |c|^2 for the recolouring cos(theta)
+__host__ __device__ constexpr float invlen(int c2) {
+    return c2 == 1 ? 1.0f : c2 == 2 ? 0.70710678118654752f : c2 == 3 ? 0.57735026918962576f : 0.0f;
+}
+
+struct FaceBC {
+    int kind;          // TSLB_BC_*
+    float u[3];        // wall velocity
+    float phi;         // colour of incoming populations (< -2: own phi); ghost phi on solid faces
+    const float* plane;  // TSLB_BC_INLET: u, v, w, phi planes of the face
+};
+
+struct StepArgs {
+    int nx, ny, nz;
+    long long N;            // field stride (floats)
+    const float* in;        // 11 fields
+    float* out;             // 11 fields
+    const float* nrm;       // phase field: interface normals (3 fields of stride N)
+    int zchunk;             // target planes per block
+    int mode;
+    float omega_pf;         // 1/tau (phase field)
+    float inv_nu_a, inv_nu_b;  // colour: 1/nu of each component
+    float sigma, beta, sharp, thr, acoef;
+    float force[3];
+    int wall_phi_mode;
+    FaceBC face[6];
+    unsigned int* flags;    // bit 0: non-finite moment produced
+};
+
+__device__ __forceinline__ long long nidx(const StepArgs& a, int x, int y, int z) {
+    return (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
+}
+__device__ __forceinline__ int wrapi(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+__device__ __forceinline__ int dimn(const StepArgs& a, int ax) { return ax == 0 ? a.nx : ax == 1 ? a.ny : a.nz; }
+
+__device__ __forceinline__ long long plane_index(const StepArgs& a, int face, int x, int y, int z) {
+    int ax = face >> 1;
+    if (ax == 0) return (long long)y + (long long)a.ny * z;
+    if (ax == 1) return (long long)x + (long long)a.nx * z;
+    return (long long)x + (long long)a.nx * y;
+}
+__device__ __forceinline__ long long plane_area(const StepArgs& a, int face) {
+    int ax = face >> 1;
+    return ax == 0 ? (long long)a.ny * a.nz : ax == 1 ? (long long)a.nx * a.nz : (long long)a.nx * a.ny;
+}
+
+// phi at any node of the halo'd lattice: periodic axes wrap; on solid faces
+// the inlet plane's phi (inlet faces), bc phi (wall_phi_mode 0) or the
+// nearest fluid value (mirror).  The first out-of-range non-periodic axis in
+// x, y, z order names the face.
+__device__ float phi_at(const StepArgs& a, int x, int y, int z) {
+    int c[3] = {x, y, z};
+    int face = -1;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        int n = dimn(a, ax);
+        if (c[ax] < 0 || c[ax] >= n) {
+            if (a.face[2 * ax].kind == TSLB_BC_PERIODIC) {
+                c[ax] = wrapi(c[ax], n);
+            } else {
+                if (face < 0) face = 2 * ax + (c[ax] >= n ? 1 : 0);
+                c[ax] = c[ax] < 0 ? 0 : n - 1;
+            }
+        }
+    }
+    if (face < 0) return __ldg(a.in + F_PHI * a.N + nidx(a, c[0], c[1], c[2]));
+    const FaceBC& fb = a.face[face];
+    if (fb.kind == TSLB_BC_INLET) return __ldg(fb.plane + 3 * plane_area(a, face) + plane_index(a, face, c[0], c[1], c[2]));
+    if (a.wall_phi_mode == 0) return fb.phi;
+    return __ldg(a.in + F_PHI * a.N + nidx(a, c[0], c[1], c[2]));
+}
+
+// normal component `comp` at any node: periodic wrap, zero on solid faces
+__device__ float nrm_at(const StepArgs& a, int comp, int x, int y, int z) {
+    int c[3] = {x, y, z};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        int n = dimn(a, ax);
+        if (c[ax] < 0 || c[ax] >= n) {
+            if (a.face[2 * ax].kind != TSLB_BC_PERIODIC) return 0.0f;
+            c[ax] = wrapi(c[ax], n);
+        }
+    }
+    return __ldg(a.nrm + comp * a.N + nidx(a, c[0], c[1], c[2]));
+}
+
+__device__ __forceinline__ bool interior1(const StepArgs& a, int x, int y, int z) {
+    return x >= 1 && x < a.nx - 1 && y >= 1 && y < a.ny - 1 && z >= 1 && z < a.nz - 1;
+}
+
+// isotropic gradient 3 sum_i p_i c_i s(x+c_i) of phi
+// (recursive_2c_TSLB3D.f90:555-565; recursive_colorTSLB3D.f90:726-744)
+__device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+    const bool fast = interior1(a, x, y, z);
+    const float* ph = a.in + F_PHI * a.N;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                const float wv = wclass(dx * dx + dy * dy + dz * dz);
+                float s = fast ? __ldg(ph + nidx(a, x + dx, y + dy, z + dz)) : phi_at(a, x + dx, y + dy, z + dz);
+                s *= wv;
+                if (dx) gx += dx > 0 ? s : -s;
+                if (dy) gy += dy > 0 ? s : -s;
+                if (dz) gz += dz > 0 ? s : -s;
+            }
+    g[0] = 3.f * gx;
+    g[1] = 3.f * gy;
+    g[2] = 3.f * gz;
+}
+
+// -div(n) with the same stencil (recursive_2c_TSLB3D.f90:617-627)
+__device__ float curvature_at(const StepArgs& a, int x, int y, int z) {
+    float div = 0.f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                const float wv = wclass(dx * dx + dy * dy + dz * dz);
+                float t = 0.f;
+                if (dx) t += dx * nrm_at(a, 0, x + dx, y + dy, z + dz);
+                if (dy) t += dy * nrm_at(a, 1, x + dx, y + dy, z + dz);
+                if (dz) t += dz * nrm_at(a, 2, x + dx, y + dy, z + dz);
+                div += wv * t;
+            }
+    return -3.f * div;
+}
+
+// Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms.
+// m[] are the node's 11 moments (m[F_D] = rho - 1).
+template <int MODE>
+__device__ void node_coefs(const StepArgs& a, const float* m, int x, int y, int z, float* K) {
+    const float d = m[F_D], rho = 1.f + d;
+    const float u = m[F_U], v = m[F_V], w = m[F_W];
+    const float pxx = m[F_XX], pxy = m[F_XY], pxz = m[F_XZ], pyy = m[F_YY], pyz = m[F_YZ], pzz = m[F_ZZ];
+    const float phi = m[F_PHI];
+    float omega, U, V, W;
+    float A = 0.f, mg = 0.f, nx_ = 0.f, ny_ = 0.f, nz_ = 0.f;
+    bool iface = false;
+    if (MODE == TSLB_MODE_COLOUR) {
+        float g[3];
+        grad_phi(a, x, y, z, g);
+        const float m2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+        mg = sqrtf(m2);
+        const float ca = 0.5f * (1.f + phi), cb = 0.5f * (1.f - phi);
+        const float nu = 1.f / (ca * a.inv_nu_a + cb * a.inv_nu_b);
+        omega = 2.f / (6.f * nu + 1.f);
+        iface = mg > a.thr;
+        if (iface) {
+            const float inv = 1.f / mg;
+            nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;
+            A = a.acoef * a.sigma * omega;
+        }
+        U = u; V = v; W = w;
+    } else {
+        omega = a.omega_pf;
+        const long long id = nidx(a, x, y, z);
+        const float n0 = __ldg(a.nrm + id), n1 = __ldg(a.nrm + a.N + id), n2 = __ldg(a.nrm + 2 * a.N + id);
+        float curv = 0.f;
+        const float ind = phi * (1.f - phi) * (n0 * n0 + n1 * n1 + n2 * n2);
+        if (ind > 0.2f) curv = curvature_at(a, x, y, z);
+        const float sk = a.sigma * curv;
+        U = u + sk * n0 + a.force[0];
+        V = v + sk * n1 + a.force[1];
+        W = w + sk * n2 + a.force[2];
+        nx_ = n0; ny_ = n1; nz_ = n2;
+    }
+    const float om1 = 1.f - omega;
+    // recursive third-order non-equilibrium moments a3 = u_a Pi_bc + perms
+    const float a_xxy = 2.f * u * pxy + v * pxx;
+    const float a_xxz = 2.f * u * pxz + w * pxx;
+    const float a_xyy = u * pyy + 2.f * v * pxy;
+    const float a_yyz = 2.f * v * pyz + w * pyy;
+    const float a_xzz = u * pzz + 2.f * w * pxz;
+    const float a_yzz = v * pzz + 2.f * w * pyz;
+    const float a_xyz = u * pyz + v * pxz + w * pxy;
+    const float UU = U * U, VV = V * V, WW = W * W;
+    const float rU = rho * U, rV = rho * V, rW = rho * W;
+    // equilibrium third-order moments rho U_a U_b U_c
+    const float e_xxy = rU * U * V, e_xxz = rU * U * W, e_xyy = rU * V * V;
+    const float e_yyz = rV * V * W, e_xzz = rU * W * W, e_yzz = rV * W * W, e_xyz = rU * V * W;
+    const float tr = pxx + pyy + pzz;
+    // full third-order coefficients (eq + (1-omega) neq)
+    const float t_xxy = e_xxy + om1 * a_xxy, t_xxz = e_xxz + om1 * a_xxz, t_xyy = e_xyy + om1 * a_xyy;
+    const float t_yyz = e_yyz + om1 * a_yyz, t_xzz = e_xzz + om1 * a_xzz, t_yzz = e_yzz + om1 * a_yzz;
+    const float t_xyz = e_xyz + om1 * a_xyz;
+    K[K_0] = d - 1.5f * rho * (UU + VV + WW) - 1.5f * om1 * tr;
+    K[K_X] = 3.f * rU - 4.5f * (t_xyy + t_xzz);
+    K[K_Y] = 3.f * rV - 4.5f * (t_xxy + t_yzz);
+    K[K_Z] = 3.f * rW - 4.5f * (t_xxz + t_yyz);
+    K[K_XX] = 4.5f * (rU * U + om1 * pxx);
+    K[K_YY] = 4.5f * (rV * V + om1 * pyy);
+    K[K_ZZ] = 4.5f * (rW * W + om1 * pzz);
+    K[K_XY] = 9.f * (rU * V + om1 * pxy);
+    K[K_XZ] = 9.f * (rU * W + om1 * pxz);
+    K[K_YZ] = 9.f * (rV * W + om1 * pyz);
+    K[K_XXY] = 13.5f * t_xxy;
+    K[K_XXZ] = 13.5f * t_xxz;
+    K[K_XYY] = 13.5f * t_xyy;
+    K[K_YYZ] = 13.5f * t_yyz;
+    K[K_XZZ] = 13.5f * t_xzz;
+    K[K_YZZ] = 13.5f * t_yzz;
+    K[K_XYZ] = 27.f * t_xyz;
+    if (MODE == TSLB_MODE_COLOUR) {
+        // force as population source 3 w c.F (recursive_colorTSLB3D.f90:776)
+        K[K_X] += 3.f * a.force[0];
+        K[K_Y] += 3.f * a.force[1];
+        K[K_Z] += 3.f * a.force[2];
+        float bx = 0.f, by = 0.f, bz = 0.f, d0 = 0.f;
+        if (iface) {
+            // perturbation (A/2)|g| [w (c.n)^2 - B_i], B_i = w_i for i >= 1
+            const float h = 0.5f * A * mg;
+            K[K_0] -= h;
+            K[K_XX] += h * nx_ * nx_;
+            K[K_YY] += h * ny_ * ny_;
+            K[K_ZZ] += h * nz_ * nz_;
+            K[K_XY] += 2.f * h * nx_ * ny_;
+            K[K_XZ] += 2.f * h * nx_ * nz_;
+            K[K_YZ] += 2.f * h * ny_ * nz_;
+            d0 = (A / 3.f) * mg;  // rest population: B_0 = -10/27 instead of w_0
+            // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta)
+            const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
+            bx = bb * nx_; by = bb * ny_; bz = bb * nz_;
+        }
+        K[K_C0] = phi; K[K_C1] = bx; K[K_C2] = by; K[K_C3] = bz; K[K_C4] = d0;
+    } else {
+        // D3Q7 phase field: g_q = G0 + e_q.G1 (recursive_2c_TSLB3D.f90:808-831)
+        const float sh = 0.125f * a.sharp * phi * (1.f - phi);
+        K[K_C0] = 0.125f * phi;
+        K[K_C1] = 0.375f * phi * u + sh * nx_;
+        K[K_C2] = 0.375f * phi * v + sh * ny_;
+        K[K_C3] = 0.375f * phi * w + sh * nz_;
+        K[K_C4] = 0.f;
+    }
+}
+
+// P'(c) for a runtime direction (boundary paths)
+__device__ __forceinline__ float eval_P(const float* K, long long stride, int cx, int cy, int cz) {
+    const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
+    const float ax = (float)(cx * cx), ay = (float)(cy * cy), az = (float)(cz * cz);
+    return K[K_0 * stride] + fx * K[K_X * stride] + fy * K[K_Y * stride] + fz * K[K_Z * stride] +
+           ax * K[K_XX * stride] + ay * K[K_YY * stride] + az * K[K_ZZ * stride] +
+           fx * fy * K[K_XY * stride] + fx * fz * K[K_XZ * stride] + fy * fz * K[K_YZ * stride] +
+           ax * fy * K[K_XXY * stride] + ax * fz * K[K_XXZ * stride] + fx * ay * K[K_XYY * stride] +
+           ay * fz * K[K_YYZ * stride] + fx * az * K[K_XZZ * stride] + fy * az * K[K_YZZ * stride] +
+           fx * fy * fz * K[K_XYZ * stride];
+}
+
+// accumulate population value f (already weighted) of direction c into acc
+template <int CXv, int CYv, int CZv>
+__device__ __forceinline__ void acc_dir(float* acc, float f) {
+    acc[A_RHO] += f;
+    if (CXv > 0) acc[A_JX] += f; else if (CXv < 0) acc[A_JX] -= f;
+    if (CYv > 0) acc[A_JY] += f; else if (CYv < 0) acc[A_JY] -= f;
+    if (CZv > 0) acc[A_JZ] += f; else if (CZv < 0) acc[A_JZ] -= f;
+    if (CXv) acc[A_XX] += f;
+    if (CYv) acc[A_YY] += f;
+    if (CZv) acc[A_ZZ] += f;
+    if (CXv * CYv > 0) acc[A_XY] += f; else if (CXv * CYv < 0) acc[A_XY] -= f;
+    if (CXv * CZv > 0) acc[A_XZ] += f; else if (CXv * CZv < 0) acc[A_XZ] -= f;
+    if (CYv * CZv > 0) acc[A_YZ] += f; else if (CYv * CZv < 0) acc[A_YZ] -= f;
+}
+
+__device__ __forceinline__ void acc_dir_rt(float* acc, int cx, int cy, int cz, float f) {
+    acc[A_RHO] += f;
+    acc[A_JX] += cx * f; acc[A_JY] += cy * f; acc[A_JZ] += cz * f;
+    acc[A_XX] += (cx * cx) * f; acc[A_YY] += (cy * cy) * f; acc[A_ZZ] += (cz * cz) * f;
+    acc[A_XY] += (cx * cy) * f; acc[A_XZ] += (cx * cz) * f; acc[A_YZ] += (cy * cz) * f;
+}
+
+}  // namespace tslb

@@ -1,0 +1,103 @@
+"""Host-side handle of one TSLB lattice on the GPU, over the C-ABI.
+
+Mirrors the reference driver's view of the state (the vars-module arrays of
+recursive_2c_TSLB3D.f90 / TSLB_2C-mpi/vars_single_3D_module.f90): fields are
+numpy arrays of shape (nz, ny, nx) in C order, which is exactly Fortran's
+column-major (1:nx,1:ny,1:nz) with x fastest.  Every method is one call
+through libtslb.so; errors raise TslbError with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+
+
+class TslbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"tslb error {code}: {msg}")
+        self.code = code
+
+
+class Lattice:
+    def __init__(self, params: capi.TslbParams, nx: int, ny: int, nz: int):
+        self.L = capi.lib()
+        self.params = params
+        self.shape = (nz, ny, nx)
+        self.n = nx * ny * nz
+        h = ctypes.c_void_p()
+        rc = self.L.tslb_create(ctypes.addressof(params), nx, ny, nz, ctypes.byref(h))
+        if rc != capi.OK:
+            raise TslbError(rc, self.L.tslb_last_error(None).decode())
+        self.h = h
+
+    # -- lifetime --------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.tslb_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != capi.OK:
+            raise TslbError(rc, self.L.tslb_last_error(self.h).decode())
+
+    # -- state -----------------------------------------------------------
+    def upload_moments(self, fields: dict) -> None:
+        arrs = [np.ascontiguousarray(fields[k], np.float32).reshape(self.shape) for k in capi.FIELDS]
+        self._check(self.L.tslb_upload_moments(self.h, *[capi.fptr(a) for a in arrs]))
+
+    def upload_pops(self, f: np.ndarray, g: np.ndarray) -> None:
+        """f: (27, nz+2, ny+2, nx+2), g: (7|27, nz+2, ny+2, nx+2) -- the reference's
+        f(0:nx+1,0:ny+1,0:nz+1,0:26) in memory order."""
+        f = np.ascontiguousarray(f, np.float32)
+        g = np.ascontiguousarray(g, np.float32)
+        self._check(self.L.tslb_upload_pops(self.h, capi.fptr(f), capi.fptr(g)))
+
+    def download(self, out: dict | None = None) -> dict:
+        if out is None:
+            out = {k: np.empty(self.shape, np.float32) for k in capi.FIELDS}
+        self._check(self.L.tslb_download_moments(self.h, *[capi.fptr(out[k]) for k in capi.FIELDS]))
+        return out
+
+    def normals(self) -> np.ndarray:
+        out = np.empty((3,) + self.shape, np.float32)
+        self._check(self.L.tslb_download_normals(self.h, capi.fptr(out[0]), capi.fptr(out[1]), capi.fptr(out[2])))
+        return out
+
+    def set_inlet(self, face: int, planes: np.ndarray) -> None:
+        planes = np.ascontiguousarray(planes, np.float32)
+        self._check(self.L.tslb_set_inlet(self.h, face, capi.fptr(planes)))
+
+    # -- time stepping ---------------------------------------------------
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.L.tslb_step(self.h, nsteps))
+
+    def synchronize(self) -> None:
+        self._check(self.L.tslb_synchronize(self.h))
+
+    def reduce(self) -> dict:
+        out = np.zeros(capi.NREDUCE, np.float64)
+        self._check(self.L.tslb_reduce(self.h, capi.dptr(out)))
+        return dict(zip(capi.RED_NAMES, out.tolist()))
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.tslb_stream(self.h) or 0)
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.tslb_launch_count(self.h))

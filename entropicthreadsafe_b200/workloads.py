@@ -1,0 +1,124 @@
+"""Initial states and parameters of the benchmark workloads.
+
+Each builder returns (params, fields) where fields holds the 11 moment
+arrays of shape (nz, ny, nx).  All noise is seeded and counter-based, so a
+workload is the same on every machine and for every rank.
+
+  droplet  64^3 fully periodic static droplet, colour gradient
+  channel  384x192x128 two-component channel: x, y periodic, bounce-back
+           walls at z, body force gx, 40 droplets of radius 8
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import capi
+
+
+def counter_uniform(seed: int, *keys: np.ndarray) -> np.ndarray:
+    """Uniform [0,1) from a splitmix64 hash of (seed, keys...), elementwise."""
+    with np.errstate(over="ignore"):
+        h = np.full(np.broadcast(*keys).shape, np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15), np.uint64)
+        for k in keys:
+            h = h ^ (np.asarray(k).astype(np.uint64) + np.uint64(0x9E3779B97F4A7C15) + (h << np.uint64(6)) + (h >> np.uint64(2)))
+            z = h + np.uint64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            h = z ^ (z >> np.uint64(31))
+    return (h >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def empty_fields(nx: int, ny: int, nz: int) -> dict:
+    f = {k: np.zeros((nz, ny, nx), np.float32) for k in capi.FIELDS}
+    f["rho"][:] = 1.0
+    return f
+
+
+def droplet(n: int = 64, radius: float = 16.0, tau: float = 0.8, sigma: float = 0.01,
+            beta: float = 0.7, width: float = 2.0):
+    """Static droplet phi = tanh((R - r)/2) at the box centre, colour mode."""
+    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=sigma, beta=beta,
+                         grad_threshold=1e-3)
+    f = empty_fields(n, n, n)
+    c = (n - 1) / 2.0  # (n+1)/2 in 1-based indices
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    r = np.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2)
+    f["phi"][:] = np.tanh((radius - r) / width)
+    return p, f
+
+
+CHANNEL = dict(nx=384, ny=192, nz=128, gx=2.5e-6, nu=0.0015, u_centre=0.05, noise=0.05,
+               ndrops=40, radius=8.0, wall_gap=12.0, sigma=0.005, beta=0.7, seed=1234)
+
+
+def droplet_centres(nx, ny, nz, ndrops, radius, wall_gap, seed, min_sep=None):
+    """Seeded rejection sampling of non-overlapping centres (periodic in x, y)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    min_sep = 2 * radius + 4 if min_sep is None else min_sep
+    zlo, zhi = wall_gap + radius, nz - 1 - wall_gap - radius
+    centres = []
+    tries = 0
+    while len(centres) < ndrops:
+        tries += 1
+        if tries > 100000:
+            raise RuntimeError("could not place droplets")
+        c = np.array([rng.uniform(0, nx), rng.uniform(0, ny), rng.uniform(zlo, zhi)])
+        ok = True
+        for q in centres:
+            dx = abs(c[0] - q[0]); dx = min(dx, nx - dx)
+            dy = abs(c[1] - q[1]); dy = min(dy, ny - dy)
+            if dx * dx + dy * dy + (c[2] - q[2]) ** 2 < min_sep ** 2:
+                ok = False
+                break
+        if ok:
+            centres.append(c)
+    return np.array(centres)
+
+
+def channel(nx: int | None = None, ny: int | None = None, nz: int | None = None, **over):
+    """Two-component channel: x, y periodic, half-way bounce-back walls at z.
+
+    The laminar profile of this force and viscosity would peak at
+    gx H^2 / (8 nu) = 3.4 lattice units, far outside the stable range, so
+    the initial mean flow is the parabolic shape scaled to u_centre = 0.05
+    (Mach 0.087), plus counter-based uniform noise of +-5% of u_centre in
+    all three components (key = (x, y, z, component), seed 1234)."""
+    cfg = dict(CHANNEL)
+    cfg.update(over)
+    nx = nx or cfg["nx"]; ny = ny or cfg["ny"]; nz = nz or cfg["nz"]
+    tau = 3 * cfg["nu"] + 0.5
+    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=cfg["sigma"], beta=cfg["beta"],
+                         grad_threshold=1e-3, force=(cfg["gx"], 0.0, 0.0),
+                         bc=[capi.BC_PERIODIC] * 4 + [capi.BC_BOUNCEBACK] * 2,
+                         bc_phi=[-1.0] * 6, wall_phi_mode=1)
+    f = empty_fields(nx, ny, nz)
+    z = (np.arange(nz) + 0.5).reshape(nz, 1, 1)
+    prof = 4.0 * z * (nz - z) / nz ** 2
+    zi, yi, xi = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    uc, amp = cfg["u_centre"], cfg["noise"] * cfg["u_centre"]
+    for comp, name in enumerate(("u", "v", "w")):
+        noise = amp * (2.0 * counter_uniform(cfg["seed"], xi, yi, zi, comp) - 1.0)
+        base = uc * prof if name == "u" else 0.0
+        f[name][:] = (base + noise).astype(np.float32)
+    cen = droplet_centres(nx, ny, nz, cfg["ndrops"], cfg["radius"], cfg["wall_gap"], cfg["seed"])
+    phi = np.full((nz, ny, nx), -1.0)
+    R = cfg["radius"]
+    for cx, cy, cz in cen:
+        # only the droplet's bounding box, with periodic images in x and y
+        for sx in (-nx, 0, nx):
+            for sy in (-ny, 0, ny):
+                x0, x1 = int(np.floor(cx + sx - R - 4)), int(np.ceil(cx + sx + R + 4))
+                y0, y1 = int(np.floor(cy + sy - R - 4)), int(np.ceil(cy + sy + R + 4))
+                z0, z1 = int(np.floor(cz - R - 4)), int(np.ceil(cz + R + 4))
+                xs = np.arange(max(x0, 0), min(x1, nx - 1) + 1)
+                ys = np.arange(max(y0, 0), min(y1, ny - 1) + 1)
+                zs = np.arange(max(z0, 0), min(z1, nz - 1) + 1)
+                if xs.size == 0 or ys.size == 0 or zs.size == 0:
+                    continue
+                Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+                r = np.sqrt((X - cx - sx) ** 2 + (Y - cy - sy) ** 2 + (Z - cz) ** 2)
+                blob = np.tanh((R - r) / 2.0)
+                sub = phi[np.ix_(zs, ys, xs)]
+                phi[np.ix_(zs, ys, xs)] = np.maximum(sub, blob)
+    f["phi"][:] = phi.astype(np.float32)
+    return p, f

@@ -1,0 +1,78 @@
+"""CPU checks of the C-ABI library: it loads, exports every declared entry
+point, and rejects bad parameters before touching the GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from entropicthreadsafe_b200 import capi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "tslb.h")
+
+
+def declared_symbols():
+    with open(HEADER) as fh:
+        text = fh.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tslb_[a-z_0-9]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from entropicthreadsafe_b200 import build
+    build.build()
+    return capi.lib()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_symbols()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_default_params_match_python_mirror(lib):
+    p = capi.TslbParams()
+    lib.tslb_default_params(ctypes.addressof(p))
+    q = capi.default_params()
+    assert ctypes.sizeof(p) == ctypes.sizeof(q)
+    assert bytes(p) == bytes(q)
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("tau_a", 0.5, capi.ERR_ARG),
+    ("tau_a", float("nan"), capi.ERR_ARG),
+    ("mode", 7, capi.ERR_ARG),
+    ("precision", capi.PREC_BF16, capi.ERR_UNSUPPORTED),
+    ("wall_phi_mode", 3, capi.ERR_ARG),
+])
+def test_create_rejects_bad_params(lib, field, value, code):
+    p = capi.default_params()
+    setattr(p, field, value)
+    h = ctypes.c_void_p()
+    rc = lib.tslb_create(ctypes.addressof(p), 8, 8, 8, ctypes.byref(h))
+    assert rc == code
+    assert not h.value
+    assert lib.tslb_last_error(None)
+
+
+def test_create_rejects_unpaired_periodic_faces(lib):
+    p = capi.default_params()
+    p.bc[4] = capi.BC_BOUNCEBACK  # z- wall, z+ periodic
+    h = ctypes.c_void_p()
+    assert lib.tslb_create(ctypes.addressof(p), 8, 8, 8, ctypes.byref(h)) == capi.ERR_ARG
+    assert b"pairs" in lib.tslb_last_error(None)
+
+
+def test_create_rejects_bad_sizes(lib):
+    p = capi.default_params()
+    h = ctypes.c_void_p()
+    assert lib.tslb_create(ctypes.addressof(p), 0, 8, 8, ctypes.byref(h)) == capi.ERR_ARG
+    assert lib.tslb_create(None, 8, 8, 8, ctypes.byref(h)) == capi.ERR_ARG
+
+
+def test_null_context_calls_fail_cleanly(lib):
+    assert lib.tslb_step(None, 1) == capi.ERR_ARG
+    assert lib.tslb_synchronize(None) == capi.ERR_ARG
+    assert lib.tslb_launch_count(None) == 0

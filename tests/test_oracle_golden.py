@@ -7,39 +7,13 @@ TSLB_2C-mpi/lb_kernels_module.f90:747-931, bounce-back
 boundary_cds_3D_module.f90:18-70 and the moving-wall condition
 boundary_cds_3D_module.f90:413-571.
 """
-import json
-import os
-
 import numpy as np
 import pytest
 
 import oracle
 from entropicthreadsafe_b200 import capi
 
-GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ("pf_periodic", "pf_walls_force", "couette")
-
-
-def golden_params(meta):
-    bc = [capi.BC_PERIODIC] * 6
-    bcu = [[0.0, 0.0, 0.0]] * 6
-    if meta["walls"] == "bounceback":
-        bc[4] = bc[5] = capi.BC_BOUNCEBACK
-    elif meta["walls"] == "couette":
-        bc[4] = bc[5] = capi.BC_VELOCITY
-        bcu = [[0, 0, 0]] * 4 + [[-meta["uwall"], 0, 0], [meta["uwall"], 0, 0]]
-    return capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=meta["tau"], sigma=meta["sigma"],
-                            sharp_c=meta["sharp_c"], force=meta["force"], bc=bc, bc_u=bcu,
-                            bc_phi=[0.0] * 6, wall_phi_mode=0)
-
-
-def load(case):
-    d = np.load(os.path.join(GOLDEN, case + ".npz"))
-    return d, json.loads(str(d["meta"]))
-
-
-def rel_err(a, b):
-    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+from helpers import GOLDEN_CASES as CASES, golden_params, load_golden as load, rel_err
 
 
 @pytest.mark.parametrize("case", CASES)
