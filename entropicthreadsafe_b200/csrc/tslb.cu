@@ -256,7 +256,6 @@ int launch_normals(tslb_ctx* c) {
     return TSLB_OK;
 }
 
-size_t step_smem() { return sizeof(float) * 2 * NCOEF * CAREA; }
 
 int launch_step(tslb_ctx* c) {
     if (c->p.mode == TSLB_MODE_PHASEFIELD) {
@@ -267,9 +266,9 @@ int launch_step(tslb_ctx* c) {
     dim3 block(TX, TY, 1);
     dim3 grid((c->nx + TX - 1) / TX, (c->ny + TY - 1) / TY, (c->nz + c->zchunk - 1) / c->zchunk);
     if (c->p.mode == TSLB_MODE_COLOUR)
-        step_kernel<TSLB_MODE_COLOUR><<<grid, block, step_smem(), c->stream>>>(a);
+        step_kernel<TSLB_MODE_COLOUR><<<grid, block, step_smem_bytes(TSLB_MODE_COLOUR), c->stream>>>(a);
     else
-        step_kernel<TSLB_MODE_PHASEFIELD><<<grid, block, step_smem(), c->stream>>>(a);
+        step_kernel<TSLB_MODE_PHASEFIELD><<<grid, block, step_smem_bytes(TSLB_MODE_PHASEFIELD), c->stream>>>(a);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
@@ -328,10 +327,11 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
         if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
     }
-    static const size_t smem = step_smem();
-    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)step_smem_bytes(TSLB_MODE_COLOUR))) != cudaSuccess)
         return bail(e, "cudaFuncSetAttribute");
-    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)step_smem_bytes(TSLB_MODE_PHASEFIELD))) != cudaSuccess)
         return bail(e, "cudaFuncSetAttribute");
     // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
     int sms = 148;

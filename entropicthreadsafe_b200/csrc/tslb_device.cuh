@@ -185,7 +185,7 @@ __device__ float curvature_at(const StepArgs& a, int x, int y, int z) {
 // Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms.
 // m[] are the node's 11 moments (m[F_D] = rho - 1).
 template <int MODE>
-__device__ void node_coefs(const StepArgs& a, const float* m, int x, int y, int z, float* K) {
+__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, int x, int y, int z, float* K) {
     const float d = m[F_D], rho = 1.f + d;
     const float u = m[F_U], v = m[F_V], w = m[F_W];
     const float pxx = m[F_XX], pxy = m[F_XY], pxz = m[F_XZ], pyy = m[F_YY], pyz = m[F_YZ], pzz = m[F_ZZ];
@@ -194,19 +194,18 @@ __device__ void node_coefs(const StepArgs& a, const float* m, int x, int y, int 
     float A = 0.f, mg = 0.f, nx_ = 0.f, ny_ = 0.f, nz_ = 0.f;
     bool iface = false;
     if (MODE == TSLB_MODE_COLOUR) {
-        float g[3];
-        grad_phi(a, x, y, z, g);
+        const float* g = gphi;
         const float m2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-        mg = sqrtf(m2);
-        const float ca = 0.5f * (1.f + phi), cb = 0.5f * (1.f - phi);
-        const float nu = 1.f / (ca * a.inv_nu_a + cb * a.inv_nu_b);
-        omega = 2.f / (6.f * nu + 1.f);
-        iface = mg > a.thr;
-        if (iface) {
-            const float inv = 1.f / mg;
-            nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;
-            A = a.acoef * a.sigma * omega;
-        }
+        iface = m2 > a.thr * a.thr;
+        const float rs = rsqrtf(m2);
+        mg = iface ? m2 * rs : 0.f;
+        // 1/nu = (rhoA/rho)/nu_a + (rhoB/rho)/nu_b ; omega = 2/(6 nu + 1) = 2q/(6 + q)
+        const float q = 0.5f * ((a.inv_nu_a + a.inv_nu_b) + phi * (a.inv_nu_a - a.inv_nu_b));
+        omega = __fdividef(2.f * q, 6.f + q);
+        // branch-free: outside the interface A = 0 and n = 0
+        const float inv = iface ? rs : 0.f;
+        nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;
+        A = iface ? a.acoef * a.sigma * omega : 0.f;
         U = u; V = v; W = w;
     } else {
         omega = a.omega_pf;
@@ -262,23 +261,19 @@ __device__ void node_coefs(const StepArgs& a, const float* m, int x, int y, int 
         K[K_X] += 3.f * a.force[0];
         K[K_Y] += 3.f * a.force[1];
         K[K_Z] += 3.f * a.force[2];
-        float bx = 0.f, by = 0.f, bz = 0.f, d0 = 0.f;
-        if (iface) {
-            // perturbation (A/2)|g| [w (c.n)^2 - B_i], B_i = w_i for i >= 1
-            const float h = 0.5f * A * mg;
-            K[K_0] -= h;
-            K[K_XX] += h * nx_ * nx_;
-            K[K_YY] += h * ny_ * ny_;
-            K[K_ZZ] += h * nz_ * nz_;
-            K[K_XY] += 2.f * h * nx_ * ny_;
-            K[K_XZ] += 2.f * h * nx_ * nz_;
-            K[K_YZ] += 2.f * h * ny_ * nz_;
-            d0 = (A / 3.f) * mg;  // rest population: B_0 = -10/27 instead of w_0
-            // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta)
-            const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
-            bx = bb * nx_; by = bb * ny_; bz = bb * nz_;
-        }
-        K[K_C0] = phi; K[K_C1] = bx; K[K_C2] = by; K[K_C3] = bz; K[K_C4] = d0;
+        // perturbation (A/2)|g| [w (c.n)^2 - B_i], B_i = w_i for i >= 1 (A = 0 off the interface)
+        const float h = 0.5f * A * mg;
+        K[K_0] -= h;
+        K[K_XX] += h * nx_ * nx_;
+        K[K_YY] += h * ny_ * ny_;
+        K[K_ZZ] += h * nz_ * nz_;
+        K[K_XY] += 2.f * h * nx_ * ny_;
+        K[K_XZ] += 2.f * h * nx_ * nz_;
+        K[K_YZ] += 2.f * h * ny_ * nz_;
+        const float d0 = (A * (1.f / 3.f)) * mg;  // rest population: B_0 = -10/27 instead of w_0
+        // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta; n = 0 off the interface)
+        const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
+        K[K_C0] = phi; K[K_C1] = bb * nx_; K[K_C2] = bb * ny_; K[K_C3] = bb * nz_; K[K_C4] = d0;
     } else {
         // D3Q7 phase field: g_q = G0 + e_q.G1 (recursive_2c_TSLB3D.f90:808-831)
         const float sh = 0.125f * a.sharp * phi * (1.f - phi);

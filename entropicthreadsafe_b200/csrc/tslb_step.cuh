@@ -23,14 +23,11 @@
 
 namespace tslb {
 
-// Populations leaving the source node whose coefficients start at Kp
-// (stride CAREA) in directions (-OX, -OY, cz), cz = -1, 0, 1.
-template <int MODE, int OX, int OY>
-__device__ __forceinline__ void pull_lateral(const float* __restrict__ Kp, float* accm, float* acc0, float* accp) {
-    constexpr int CXv = -OX, CYv = -OY;
-    constexpr int AX = CXv * CXv, AY = CYv * CYv;
+// P'(c) of one source node for the directions (CXv, CYv, cz), cz = -1, 0, 1:
+// P' = Q0 + cz Q1 + cz^2 Q2 with the node's coefficients at Kp (stride CAREA).
+template <int CXv, int CYv>
+__device__ __forceinline__ void eval_lateral(const float* __restrict__ Kp, float& Pm, float& P0, float& Pp) {
     auto L = [&](int slot) { return Kp[slot * CAREA]; };
-    // P'(cx,cy,cz) = Q0 + cz Q1 + cz^2 Q2
     float q0 = L(K_0);
     if (CXv) q0 += CXv * L(K_X) + L(K_XX);
     if (CYv) q0 += CYv * L(K_Y) + L(K_YY);
@@ -43,38 +40,91 @@ __device__ __forceinline__ void pull_lateral(const float* __restrict__ Kp, float
     if (CXv) q2 += CXv * L(K_XZZ);
     if (CYv) q2 += CYv * L(K_YZZ);
     const float t = q0 + q2;
-    const float Pm = t - q1, P0 = q0, Pp = t + q1;   // cz = -1, 0, +1
-    constexpr float w0 = wclass(AX + AY), w1 = wclass(AX + AY + 1);
-    const float fm = w1 * Pm, f0 = w0 * P0, fp = w1 * Pp;
-    acc_dir<CXv, CYv, -1>(accm, fm);
-    acc_dir<CXv, CYv, 0>(acc0, f0);
-    acc_dir<CXv, CYv, 1>(accp, fp);
+    Pm = t - q1;
+    P0 = q0;
+    Pp = t + q1;
+}
+
+__host__ __device__ constexpr float w1d(int c) { return c == 0 ? 2.0f / 3.0f : 1.0f / 6.0f; }
+
+// Moments of the three populations of one (cy, cz) group: directions
+// (+1, cy, cz), (0, cy, cz), (-1, cy, cz) with values a, c0, b (unweighted
+// P'), folded through S = a + b and D = a - b before accumulation.
+template <int CYv, int CZv>
+__device__ __forceinline__ void acc_group(float* acc, float a, float c0, float b) {
+    constexpr float wE = w1d(1) * w1d(CYv) * w1d(CZv), wC = w1d(0) * w1d(CYv) * w1d(CZv);
+    const float S = wE * (a + b), D = wE * (a - b), T = fmaf(wC, c0, S);
+    acc[A_RHO] += T;
+    acc[A_JX] += D;
+    acc[A_XX] += S;
+    if (CYv) { acc[A_JY] += CYv > 0 ? T : -T; acc[A_YY] += T; acc[A_XY] += CYv > 0 ? D : -D; }
+    if (CZv) { acc[A_JZ] += CZv > 0 ? T : -T; acc[A_ZZ] += T; acc[A_XZ] += CZv > 0 ? D : -D; }
+    if (CYv && CZv) acc[A_YZ] += (CYv * CZv) > 0 ? T : -T;
+}
+
+// colour of one (cy, cz) group: w (phi (1 + P') + (B.c)/|c|) summed over cx
+template <int CYv, int CZv>
+__device__ __forceinline__ void col_group(float* acc, float ha, float hc, float hb, float Ex, float Ey, float Ez,
+                                          float By0, float Bz0) {
+    constexpr int cE = 1 + CYv * CYv + CZv * CZv, cC = CYv * CYv + CZv * CZv;
+    constexpr float wE = w1d(1) * w1d(CYv) * w1d(CZv), wC = w1d(0) * w1d(CYv) * w1d(CZv);
+    float r = Ex;
+    if (CYv) r += CYv > 0 ? Ey : -Ey;
+    if (CZv) r += CZv > 0 ? Ez : -Ez;
+    float v = fmaf(wE, ha + hb, wC * hc);
+    v = fmaf(wE * invlen(cE), r, v);
+    if (cC) {
+        float rc = 0.f;
+        if (CYv) rc += CYv > 0 ? By0 : -By0;
+        if (CZv) rc += CZv > 0 ? Bz0 : -Bz0;
+        v = fmaf(wC * invlen(cC), rc, v);
+    }
+    acc[A_COL] += v;
+}
+
+// All populations that leave the source row y - CYv of plane s and land on
+// the column's targets in planes s-1 (accm), s (acc0), s+1 (accp).  Kc
+// points at the column's own node in the coefficient tile.
+template <int MODE, int CYv>
+__device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp) {
+    const float* Ka = Kc - CYv * CW - 1;  // source of cx = +1 (x - 1)
+    const float* Kz = Kc - CYv * CW;      // source of cx = 0
+    const float* Kb = Kc - CYv * CW + 1;  // source of cx = -1 (x + 1)
+    float am, a0, ap, cm, c0, cp, bm, b0, bp;
+    eval_lateral<1, CYv>(Ka, am, a0, ap);
+    eval_lateral<0, CYv>(Kz, cm, c0, cp);
+    eval_lateral<-1, CYv>(Kb, bm, b0, bp);
+    acc_group<CYv, -1>(accm, am, cm, bm);
+    acc_group<CYv, 0>(acc0, a0, c0, b0);
+    acc_group<CYv, 1>(accp, ap, cp, bp);
     if (MODE == TSLB_MODE_COLOUR) {
-        // colour: w (phi (1 + P') + (B.c)/|c|); rest population adds delta0
-        const float ph = L(K_C0);
-        const float bl = (CXv ? CXv * L(K_C1) : 0.f) + (CYv ? CYv * L(K_C2) : 0.f);
-        const float bz = L(K_C3);
-        constexpr float il0 = invlen(AX + AY), il1 = invlen(AX + AY + 1);
-        accm[A_COL] += w1 * fmaf(ph, Pm, ph) + (w1 * il1) * (bl - bz);
-        accp[A_COL] += w1 * fmaf(ph, Pp, ph) + (w1 * il1) * (bl + bz);
-        if (AX + AY == 0) {
-            const float d0 = L(K_C4);
+        const float pa = Ka[K_C0 * CAREA], pz = Kz[K_C0 * CAREA], pb = Kb[K_C0 * CAREA];
+        // recolouring sums over the cx = +1 / -1 sources
+        const float Ex = Ka[K_C1 * CAREA] - Kb[K_C1 * CAREA];
+        const float Ey = CYv ? Ka[K_C2 * CAREA] + Kb[K_C2 * CAREA] : 0.f;
+        const float Ez = Ka[K_C3 * CAREA] + Kb[K_C3 * CAREA];
+        const float By0 = CYv ? Kz[K_C2 * CAREA] : 0.f;
+        const float Bz0 = Kz[K_C3 * CAREA];
+        col_group<CYv, -1>(accm, fmaf(pa, am, pa), fmaf(pz, cm, pz), fmaf(pb, bm, pb), Ex, Ey, Ez, By0, Bz0);
+        col_group<CYv, 0>(acc0, fmaf(pa, a0, pa), fmaf(pz, c0, pz), fmaf(pb, b0, pb), Ex, Ey, Ez, By0, Bz0);
+        col_group<CYv, 1>(accp, fmaf(pa, ap, pa), fmaf(pz, cp, pz), fmaf(pb, bp, pb), Ex, Ey, Ez, By0, Bz0);
+        if (CYv == 0) {
+            // rest population: f_0 += delta0 (perturbation with B_0 = -10/27)
+            const float d0 = Kz[K_C4 * CAREA];
             acc0[A_RHO] += d0;
-            acc0[A_COL] += w0 * fmaf(ph, P0, ph) + ph * d0;
-        } else {
-            acc0[A_COL] += w0 * fmaf(ph, P0, ph) + (w0 * il0) * bl;
+            acc0[A_COL] = fmaf(pz, d0, acc0[A_COL]);
         }
     } else {
-        // phase field g: axis directions and the rest population only
-        if (AX + AY == 0) {
-            const float g0 = L(K_C0), gz = L(K_C3);
-            accm[A_COL] += g0 - gz;      // q = 6 (-z) leaves the source below... direction (0,0,-1)
-            accp[A_COL] += g0 + gz;      // q = 5 (+z)
-            acc0[A_COL] += 2.f * g0;     // q = 0: p0g phi = 2 G0
-        } else if (AX + AY == 1) {
-            const float g0 = L(K_C0);
-            const float ge = CXv ? CXv * L(K_C1) : CYv * L(K_C2);
-            acc0[A_COL] += g0 + ge;
+        // phase field g (D3Q7): axis directions and the rest population
+        if (CYv == 0) {
+            const float g0 = Kz[K_C0 * CAREA], gz = Kz[K_C3 * CAREA];
+            accm[A_COL] += g0 - gz;   // q = 6, (0,0,-1)
+            accp[A_COL] += g0 + gz;   // q = 5, (0,0,+1)
+            acc0[A_COL] += Ka[K_C0 * CAREA] + Ka[K_C1 * CAREA];   // q = 1 from x - 1
+            acc0[A_COL] += Kb[K_C0 * CAREA] - Kb[K_C1 * CAREA];   // q = 2 from x + 1
+            acc0[A_COL] = fmaf(2.f, g0, acc0[A_COL]);            // q = 0: p0g phi = 2 G0
+        } else {
+            acc0[A_COL] += Kz[K_C0 * CAREA] + CYv * Kz[K_C2 * CAREA];  // q = 3 / 4
         }
     }
 }
@@ -141,7 +191,12 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
                 phib = m[F_PHI];
             }
             float Uf[3] = {Ub[0], Ub[1], Ub[2]};  // velocity of the f equilibrium
-            if (fb.kind == TSLB_BC_OUTLET) Uf[ax] = m[F_U + ax];
+            if (fb.kind == TSLB_BC_OUTLET) {
+                // outlet: the normal velocity of the fluid node (zero gradient)
+                if (ax == 0) Uf[0] = m[F_U];
+                else if (ax == 1) Uf[1] = m[F_V];
+                else Uf[2] = m[F_W];
+            }
             const float d = m[F_D], rho = 1.f + d;
             float omega;
             if (MODE == TSLB_MODE_COLOUR) {
@@ -185,9 +240,77 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
     }
 }
 
+// phi tile of a plane with a two-node halo (the gradient of the halo
+// coefficient nodes reaches two nodes out)
+constexpr int PW = TX + 4, PH = TY + 4, PAREA = PW * PH;
+constexpr int NTHR = TX * TY;
+constexpr int NHALO = CAREA - NTHR;          // coefficient nodes on the tile rim (84)
+constexpr int NPHI_ROUNDS = (PAREA + NTHR - 1) / NTHR;
+
+__host__ __device__ constexpr size_t step_smem_bytes(int mode) {
+    return sizeof(float) * (2 * NCOEF * CAREA + 2 * (NF - 1) * CAREA + (mode == TSLB_MODE_COLOUR ? 4 * PAREA : 0));
+}
+
+// gradient 3 sum_i p_i c_i phi(x+c_i) from three phi planes held in shared
+// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch PW)
+__device__ __forceinline__ void grad_smem(const float* pm, const float* p0, const float* pp, float g[3]) {
+    // x: +x face minus -x face, grouped by weight class
+    auto P = [&](const float* pl, int dx, int dy) { return pl[dy * PW + dx]; };
+    const float x1 = P(p0, 1, 0) - P(p0, -1, 0);
+    const float x2 = (P(p0, 1, 1) + P(p0, 1, -1) + P(pp, 1, 0) + P(pm, 1, 0)) -
+                     (P(p0, -1, 1) + P(p0, -1, -1) + P(pp, -1, 0) + P(pm, -1, 0));
+    const float x3 = (P(pp, 1, 1) + P(pp, 1, -1) + P(pm, 1, 1) + P(pm, 1, -1)) -
+                     (P(pp, -1, 1) + P(pp, -1, -1) + P(pm, -1, 1) + P(pm, -1, -1));
+    const float y1 = P(p0, 0, 1) - P(p0, 0, -1);
+    const float y2 = (P(p0, 1, 1) + P(p0, -1, 1) + P(pp, 0, 1) + P(pm, 0, 1)) -
+                     (P(p0, 1, -1) + P(p0, -1, -1) + P(pp, 0, -1) + P(pm, 0, -1));
+    const float y3 = (P(pp, 1, 1) + P(pp, -1, 1) + P(pm, 1, 1) + P(pm, -1, 1)) -
+                     (P(pp, 1, -1) + P(pp, -1, -1) + P(pm, 1, -1) + P(pm, -1, -1));
+    const float z1 = P(pp, 0, 0) - P(pm, 0, 0);
+    const float z2 = (P(pp, 1, 0) + P(pp, -1, 0) + P(pp, 0, 1) + P(pp, 0, -1)) -
+                     (P(pm, 1, 0) + P(pm, -1, 0) + P(pm, 0, 1) + P(pm, 0, -1));
+    const float z3 = (P(pp, 1, 1) + P(pp, 1, -1) + P(pp, -1, 1) + P(pp, -1, -1)) -
+                     (P(pm, 1, 1) + P(pm, 1, -1) + P(pm, -1, 1) + P(pm, -1, -1));
+    constexpr float c1 = 3.f * wclass(1), c2 = 3.f * wclass(2), c3 = 3.f * wclass(3);
+    g[0] = c1 * x1 + c2 * x2 + c3 * x3;
+    g[1] = c1 * y1 + c2 * y2 + c3 * y3;
+    g[2] = c1 * z1 + c2 * z2 + c3 * z3;
+}
+
+// Node descriptor: in-plane offset after the periodic wrap of x and y, and
+// whether the node lies behind a non-periodic x or y face.
+struct XYNode {
+    int off;      // gx + nx * gy (wrapped/clamped)
+    int gx, gy;   // raw coordinates (may be out of range)
+    bool out;     // behind a non-periodic x or y face
+};
+
+__device__ __forceinline__ XYNode xy_node(const StepArgs& a, int gx, int gy, bool xper, bool yper) {
+    XYNode n;
+    n.gx = gx; n.gy = gy; n.out = false;
+    int cx = gx, cy = gy;
+    if (cx < 0 || cx >= a.nx) { if (xper) cx = wrapi(cx, a.nx); else { n.out = true; cx = cx < 0 ? 0 : a.nx - 1; } }
+    if (cy < 0 || cy >= a.ny) { if (yper) cy = wrapi(cy, a.ny); else { n.out = true; cy = cy < 0 ? 0 : a.ny - 1; } }
+    n.off = cx + a.nx * cy;
+    return n;
+}
+
+__device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+constexpr int NMOM = NF - 1;  // moments staged per coefficient node (phi comes from the phi ring)
+
 template <int MODE>
-__global__ void __launch_bounds__(TX * TY, 2) step_kernel(const StepArgs a) {
-    extern __shared__ float smem[];  // 2 buffers x NCOEF x CAREA
+__global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
+    extern __shared__ float smem[];
+    float* coef_base = smem;                          // [2][NCOEF][CAREA]
+    float* mst = coef_base + 2 * NCOEF * CAREA;       // [2][NMOM][CAREA] staged moments
+    float* phis = mst + 2 * NMOM * CAREA;             // colour: [4][PAREA] ring of phi planes
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * a.zchunk;
@@ -197,6 +320,8 @@ __global__ void __launch_bounds__(TX * TY, 2) step_kernel(const StepArgs a) {
     const bool xper = a.face[0].kind == TSLB_BC_PERIODIC;
     const bool yper = a.face[2].kind == TSLB_BC_PERIODIC;
     const bool zper = a.face[4].kind == TSLB_BC_PERIODIC;
+    const long long plane = (long long)a.nx * a.ny;
+
     // faces the column touches (z faces are added per plane)
     unsigned colmask = 0;
     if (active) {
@@ -206,52 +331,137 @@ __global__ void __launch_bounds__(TX * TY, 2) step_kernel(const StepArgs a) {
         if (!yper && Y == a.ny - 1) colmask |= 8u;
     }
 
+    // coefficient nodes of this thread: its own column, and one rim node
+    XYNode cn[2];
+    int cidx[2];
+    cn[0] = xy_node(a, X, Y, xper, yper);
+    cidx[0] = (ty + 1) * CW + (tx + 1);
+    const bool has_rim = tid < NHALO;
+    {
+        int h = has_rim ? tid : 0, cx, cy;
+        if (h < CW) { cx = h; cy = 0; }
+        else if (h < 2 * CW) { cx = h - CW; cy = CH - 1; }
+        else if (h < 2 * CW + TY) { cx = 0; cy = h - 2 * CW + 1; }
+        else { cx = CW - 1; cy = h - 2 * CW - TY + 1; }
+        cn[1] = xy_node(a, x0 - 1 + cx, y0 - 1 + cy, xper, yper);
+        cidx[1] = cy * CW + cx;
+    }
+    const int nnodes = has_rim ? 2 : 1;
+    int pidx[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) pidx[r] = (cidx[r] / CW + 1) * PW + (cidx[r] % CW + 1);
+    // phi nodes this thread stages (colour mode)
+    XYNode pn[NPHI_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < NPHI_ROUNDS; ++r) {
+        int j = tid + r * NTHR;
+        j = j < PAREA ? j : 0;
+        pn[r] = xy_node(a, x0 - 2 + j % PW, y0 - 2 + j / PW, xper, yper);
+    }
+
+    auto zwrap = [&](int z, bool& out) {
+        out = false;
+        if (z < 0 || z >= a.nz) { if (zper) return wrapi(z, a.nz); out = true; }
+        return z;
+    };
+    // stage phi of plane z into ring slot z & 3 (asynchronous copies, ghost
+    // values computed)
+    auto stage_phi = [&](int z) {
+        bool zout;
+        const int gz = zwrap(z, zout);
+        float* slot = phis + (z & 3) * PAREA;
+        const float* ph = a.in + F_PHI * a.N + (long long)gz * plane;
+#pragma unroll
+        for (int r = 0; r < NPHI_ROUNDS; ++r) {
+            const int j = tid + r * NTHR;
+            if (j < PAREA) {
+                if (!pn[r].out && !zout) cp_async4(slot + j, ph + pn[r].off);
+                else slot[j] = phi_at(a, pn[r].gx, pn[r].gy, z);
+            }
+        }
+    };
+    // stage the 10 non-phi moments of this thread's coefficient nodes of plane z
+    auto stage_mom = [&](int z) {
+        bool zout;
+        const int gz = zwrap(z, zout);
+        if (zout) return;
+        float* dst = mst + (z & 1) * (NMOM * CAREA);
+        const float* src = a.in + (long long)gz * plane;
+        for (int r = 0; r < nnodes; ++r) {
+            const XYNode nd = r ? cn[1] : cn[0];
+            if (nd.out) continue;
+            const float* p = src + nd.off;
+            float* d = dst + (r ? cidx[1] : cidx[0]);
+#pragma unroll
+            for (int f = 0; f < NMOM; ++f) cp_async4(d + f * CAREA, p + f * a.N);
+        }
+    };
+
+    if (MODE == TSLB_MODE_COLOUR) {
+        stage_phi(z0 - 2);
+        stage_phi(z0 - 1);
+        stage_phi(z0);
+    }
+    stage_mom(z0 - 1);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
     float accm[NACC], acc0[NACC], accp[NACC];
 #pragma unroll
     for (int i = 0; i < NACC; ++i) { accm[i] = 0.f; acc0[i] = 0.f; accp[i] = 0.f; }
 
     int buf = 0;
     for (int s = z0 - 1; s <= z1; ++s) {
-        float* coef = smem + buf * (NCOEF * CAREA);
-        // ---- 1. coefficients of source plane s (tile + halo) ----
-        int gz = s;
-        bool zsolid = false;
-        if (gz < 0 || gz >= a.nz) {
-            if (zper) gz = wrapi(gz, a.nz); else zsolid = true;
-        }
-        for (int idx = tid; idx < CAREA; idx += TX * TY) {
-            const int cyy = idx / CW, cxx = idx - cyy * CW;
-            int gx = x0 - 1 + cxx, gy = y0 - 1 + cyy;
-            bool solid = zsolid;
-            if (gx < 0 || gx >= a.nx) { if (xper) gx = wrapi(gx, a.nx); else solid = true; }
-            if (gy < 0 || gy >= a.ny) { if (yper) gy = wrapi(gy, a.ny); else solid = true; }
+        float* coef = coef_base + buf * (NCOEF * CAREA);
+        const bool more = s < z1;
+        // ---- 0. prefetch: phi of plane s+2, moments of plane s+1 ----
+        if (MODE == TSLB_MODE_COLOUR && more) stage_phi(s + 2);
+        cp_async_commit();
+        if (more) stage_mom(s + 1);
+        cp_async_commit();
+        cp_async_wait<2>();  // this thread's moments of plane s have landed
+        // ---- 1. coefficients of source plane s: own column and one rim node ----
+        bool zsolid;
+        const int gz = zwrap(s, zsolid);
+        const float* ms = mst + (s & 1) * (NMOM * CAREA);
+        for (int r = 0; r < nnodes; ++r) {
+            const XYNode nd = r ? cn[1] : cn[0];
+            const int ci = r ? cidx[1] : cidx[0];
+            const int pi = r ? pidx[1] : pidx[0];
             float K[NCOEF];
-            if (solid) {
+            if (zsolid || nd.out) {
 #pragma unroll
                 for (int c = 0; c < NCOEF; ++c) K[c] = 0.f;
             } else {
                 float m[NF];
-                const long long id = nidx(a, gx, gy, gz);
 #pragma unroll
-                for (int f = 0; f < NF; ++f) m[f] = __ldg(a.in + f * a.N + id);
-                node_coefs<MODE>(a, m, gx, gy, gz, K);
+                for (int f = 0; f < NMOM; ++f) m[f] = ms[f * CAREA + ci];
+                float g[3] = {0.f, 0.f, 0.f};
+                if (MODE == TSLB_MODE_COLOUR) {
+                    const float* p0 = phis + (s & 3) * PAREA + pi;
+                    const float* pm = phis + ((s - 1) & 3) * PAREA + pi;
+                    const float* pp = phis + ((s + 1) & 3) * PAREA + pi;
+                    m[F_PHI] = *p0;
+                    grad_smem(pm, p0, pp, g);
+                } else {
+                    m[F_PHI] = __ldg(a.in + F_PHI * a.N + (long long)gz * plane + nd.off);
+                }
+                const int gx = nd.off % a.nx, gy = nd.off / a.nx;
+                node_coefs<MODE>(a, m, g, gx, gy, gz, K);
             }
+            float* dst = coef + ci;
 #pragma unroll
-            for (int c = 0; c < NCOEF; ++c) coef[c * CAREA + idx] = K[c];
+            for (int c = 0; c < NCOEF; ++c) dst[c * CAREA] = K[c];
         }
+        cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
         // ---- 2. pull ----
         if (active) {
             const float* Kc = coef + (ty + 1) * CW + (tx + 1);
-            pull_lateral<MODE, -1, -1>(Kc - CW - 1, accm, acc0, accp);
-            pull_lateral<MODE, 0, -1>(Kc - CW, accm, acc0, accp);
-            pull_lateral<MODE, 1, -1>(Kc - CW + 1, accm, acc0, accp);
-            pull_lateral<MODE, -1, 0>(Kc - 1, accm, acc0, accp);
-            pull_lateral<MODE, 0, 0>(Kc, accm, acc0, accp);
-            pull_lateral<MODE, 1, 0>(Kc + 1, accm, acc0, accp);
-            pull_lateral<MODE, -1, 1>(Kc + CW - 1, accm, acc0, accp);
-            pull_lateral<MODE, 0, 1>(Kc + CW, accm, acc0, accp);
-            pull_lateral<MODE, 1, 1>(Kc + CW + 1, accm, acc0, accp);
+            pull_row<MODE, -1>(Kc, accm, acc0, accp);
+            pull_row<MODE, 0>(Kc, accm, acc0, accp);
+            pull_row<MODE, 1>(Kc, accm, acc0, accp);
             // ---- 3. populations from behind non-periodic faces, target plane s ----
             if (s >= z0 && s < z1) {
                 unsigned mask = colmask;
@@ -275,11 +485,11 @@ __global__ void __launch_bounds__(TX * TY, 2) step_kernel(const StepArgs a) {
                 o[F_XZ] = accm[A_XZ] - rho * u * w;
                 o[F_YZ] = accm[A_YZ] - rho * v * w;
                 o[F_PHI] = MODE == TSLB_MODE_COLOUR ? accm[A_COL] * inv : accm[A_COL];
-                const long long id = nidx(a, X, Y, t);
+                float* po = a.out + (long long)t * plane + cn[0].off;
                 float chk = 0.f;
 #pragma unroll
                 for (int f = 0; f < NF; ++f) {
-                    a.out[f * a.N + id] = o[f];
+                    po[f * a.N] = o[f];
                     chk += o[f];
                 }
                 if (!isfinite(chk)) atomicOr(a.flags, 1u);
@@ -290,6 +500,7 @@ __global__ void __launch_bounds__(TX * TY, 2) step_kernel(const StepArgs a) {
         for (int i = 0; i < NACC; ++i) { accm[i] = acc0[i]; acc0[i] = accp[i]; accp[i] = 0.f; }
         buf ^= 1;
     }
+    cp_async_wait<0>();
 }
 
 }  // namespace tslb
