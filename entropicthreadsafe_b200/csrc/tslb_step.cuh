@@ -62,7 +62,9 @@ __device__ __forceinline__ void acc_group(float* acc, float a, float c0, float b
     if (CYv && CZv) acc[A_YZ] += (CYv * CZv) > 0 ? T : -T;
 }
 
-// colour of one (cy, cz) group: w (phi (1 + P') + (B.c)/|c|) summed over cx
+// colour of one (cy, cz) group, as an increment over the target's own
+// phi: w ((phi_s - phi_t)(1 + P') + (B.c)/|c|) summed over cx.  Uniform
+// colour regions then keep phi exactly.
 template <int CYv, int CZv>
 __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float hb, float Ex, float Ey, float Ez,
                                           float By0, float Bz0) {
@@ -86,7 +88,8 @@ __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float 
 // the column's targets in planes s-1 (accm), s (acc0), s+1 (accp).  Kc
 // points at the column's own node in the coefficient tile.
 template <int MODE, int CYv>
-__device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp) {
+__device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp,
+                                         float phm, float ph0, float php) {
     const float* Ka = Kc - CYv * CW - 1;  // source of cx = +1 (x - 1)
     const float* Kz = Kc - CYv * CW;      // source of cx = 0
     const float* Kb = Kc - CYv * CW + 1;  // source of cx = -1 (x + 1)
@@ -105,14 +108,15 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
         const float Ez = Ka[K_C3 * CAREA] + Kb[K_C3 * CAREA];
         const float By0 = CYv ? Kz[K_C2 * CAREA] : 0.f;
         const float Bz0 = Kz[K_C3 * CAREA];
-        col_group<CYv, -1>(accm, fmaf(pa, am, pa), fmaf(pz, cm, pz), fmaf(pb, bm, pb), Ex, Ey, Ez, By0, Bz0);
-        col_group<CYv, 0>(acc0, fmaf(pa, a0, pa), fmaf(pz, c0, pz), fmaf(pb, b0, pb), Ex, Ey, Ez, By0, Bz0);
-        col_group<CYv, 1>(accp, fmaf(pa, ap, pa), fmaf(pz, cp, pz), fmaf(pb, bp, pb), Ex, Ey, Ez, By0, Bz0);
+        // (phi_s - phi_t)(1 + P') for the three sources and the three target planes
+        auto h = [](float ps, float pt, float P) { const float d = ps - pt; return fmaf(d, P, d); };
+        col_group<CYv, -1>(accm, h(pa, phm, am), h(pz, phm, cm), h(pb, phm, bm), Ex, Ey, Ez, By0, Bz0);
+        col_group<CYv, 0>(acc0, h(pa, ph0, a0), h(pz, ph0, c0), h(pb, ph0, b0), Ex, Ey, Ez, By0, Bz0);
+        col_group<CYv, 1>(accp, h(pa, php, ap), h(pz, php, cp), h(pb, php, bp), Ex, Ey, Ez, By0, Bz0);
         if (CYv == 0) {
-            // rest population: f_0 += delta0 (perturbation with B_0 = -10/27)
-            const float d0 = Kz[K_C4 * CAREA];
-            acc0[A_RHO] += d0;
-            acc0[A_COL] = fmaf(pz, d0, acc0[A_COL]);
+            // rest population: f_0 += delta0 (perturbation with B_0 = -10/27); its
+            // colour is the target's own, so it adds no colour increment
+            acc0[A_RHO] += Kz[K_C4 * CAREA];
         }
     } else {
         // phase field g (D3Q7): axis directions and the rest population
@@ -133,6 +137,8 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 // behind non-periodic faces; Kp points at the target's own coefficients.
 template <int MODE>
 __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp, unsigned mask, int x, int y, int z, float* acc) {
+    // colour mode accumulates colour increments over the target's own phi
+    const float pht = Kp[K_C0 * CAREA];
     // own raw moments (velocity faces only)
     float m[NF];
     bool have_m = false;
@@ -158,14 +164,22 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
         if (!solid) continue;
         const int c2 = dx * dx + dy * dy + dz * dz;
         const float wq = wclass(c2);
+        if (MODE == TSLB_MODE_COLOUR) {
+            // The pull skips whole solid z planes, but a source behind an x or y
+            // face is a zero-coefficient node that added w (0 - phi_t): undo it.
+            const bool xy_solid = (dx && (mask & (1u << (dx > 0 ? 0 : 1)))) || (dy && (mask & (1u << (dy > 0 ? 2 : 3))));
+            const int sz = z - dz;
+            const bool zplane_solid = a.face[4].kind != TSLB_BC_PERIODIC && (sz < 0 || sz >= a.nz);
+            if (xy_solid && !zplane_solid) acc[A_COL] += wq * pht;
+        }
         if (vface < 0) {
             // half-way bounce-back: f_c(x) = f^post_{-c}(x)
             const float P = eval_P(Kp, CAREA, -dx, -dy, -dz);
             acc_dir_rt(acc, dx, dy, dz, wq * P);
             if (MODE == TSLB_MODE_COLOUR) {
-                const float ph = Kp[K_C0 * CAREA];
+                // the reflected population carries the target's own colour: only the recolouring term
                 const float bc = -(dx * Kp[K_C1 * CAREA] + dy * Kp[K_C2 * CAREA] + dz * Kp[K_C3 * CAREA]);
-                acc[A_COL] += wq * fmaf(ph, P, ph) + wq * invlen(c2) * bc;
+                acc[A_COL] += wq * invlen(c2) * bc;
             } else if (c2 == 1) {
                 const float ge = -(dx * Kp[K_C1 * CAREA] + dy * Kp[K_C2 * CAREA] + dz * Kp[K_C3 * CAREA]);
                 acc[A_COL] += Kp[K_C0 * CAREA] + ge;
@@ -230,7 +244,8 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
             const float P = feqm1 + (1.f - omega) * an;
             acc_dir_rt(acc, dx, dy, dz, wq * P);
             if (MODE == TSLB_MODE_COLOUR) {
-                acc[A_COL] += wq * fmaf(phib, P, phib);
+                const float dphi = phib - pht;
+                acc[A_COL] += wq * fmaf(dphi, P, dphi);
             } else if (c2 == 1) {
                 // g entering from the face (:984-986, :1044-1045)
                 const float eu = dx * Ub[0] + dy * Ub[1] + dz * Ub[2];
@@ -425,12 +440,13 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         bool zsolid;
         const int gz = zwrap(s, zsolid);
         const float* ms = mst + (s & 1) * (NMOM * CAREA);
-        for (int r = 0; r < nnodes; ++r) {
+        // a solid source plane sends nothing: no coefficients, no pull
+        for (int r = 0; r < (zsolid ? 0 : nnodes); ++r) {
             const XYNode nd = r ? cn[1] : cn[0];
             const int ci = r ? cidx[1] : cidx[0];
             const int pi = r ? pidx[1] : pidx[0];
             float K[NCOEF];
-            if (zsolid || nd.out) {
+            if (nd.out) {
 #pragma unroll
                 for (int c = 0; c < NCOEF; ++c) K[c] = 0.f;
             } else {
@@ -459,9 +475,19 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         // ---- 2. pull ----
         if (active) {
             const float* Kc = coef + (ty + 1) * CW + (tx + 1);
-            pull_row<MODE, -1>(Kc, accm, acc0, accp);
-            pull_row<MODE, 0>(Kc, accm, acc0, accp);
-            pull_row<MODE, 1>(Kc, accm, acc0, accp);
+            float phm = 0.f, ph0 = 0.f, php = 0.f;
+            if (MODE == TSLB_MODE_COLOUR) {
+                // own-column phi of the target planes (the ring holds planes s-1 .. s+2)
+                const int po = (ty + 2) * PW + (tx + 2);
+                phm = phis[((s - 1) & 3) * PAREA + po];
+                ph0 = phis[(s & 3) * PAREA + po];
+                php = phis[((s + 1) & 3) * PAREA + po];
+            }
+            if (!zsolid) {
+                pull_row<MODE, -1>(Kc, accm, acc0, accp, phm, ph0, php);
+                pull_row<MODE, 0>(Kc, accm, acc0, accp, phm, ph0, php);
+                pull_row<MODE, 1>(Kc, accm, acc0, accp, phm, ph0, php);
+            }
             // ---- 3. populations from behind non-periodic faces, target plane s ----
             if (s >= z0 && s < z1) {
                 unsigned mask = colmask;
@@ -484,7 +510,8 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
                 o[F_XY] = accm[A_XY] - rho * u * v;
                 o[F_XZ] = accm[A_XZ] - rho * u * w;
                 o[F_YZ] = accm[A_YZ] - rho * v * w;
-                o[F_PHI] = MODE == TSLB_MODE_COLOUR ? accm[A_COL] * inv : accm[A_COL];
+                // colour mode: phi_t + (colour increment) / rho
+                o[F_PHI] = MODE == TSLB_MODE_COLOUR ? fmaf(accm[A_COL], inv, phm) : accm[A_COL];
                 float* po = a.out + (long long)t * plane + cn[0].off;
                 float chk = 0.f;
 #pragma unroll

@@ -145,3 +145,25 @@ def test_reduce_is_exact_and_matches_oracle():
             assert abs(rg[name] - ro[k]) <= 1e-5 * max(1.0, abs(ro[k])), name
         elif name in ("kinetic", "umax", "dp"):
             assert abs(rg[name] - ro[k]) <= 1e-2 * abs(ro[k]) + 1e-12, name
+
+
+def test_uniform_colour_is_kept_exactly():
+    """A single-colour flow (phi = -1 everywhere) keeps phi bit-exactly: the
+    colour update is an increment that vanishes where phi is uniform."""
+    p, f = workloads.channel(nx=40, ny=24, nz=20, ndrops=0, gx=2.5e-5)
+    f["phi"][:] = -1.0
+    gpu, _ = run_gpu(p, f, 50)
+    assert np.all(gpu["phi"] == -1.0)
+
+
+def test_colour_droplet_bounceback_all_faces():
+    """Walls on x, y and z faces (lateral solid sources and solid planes)."""
+    p, f = workloads.droplet(n=20, radius=5.0, tau=0.9, sigma=0.01, beta=0.7)
+    for face in range(6):
+        p.bc[face] = capi.BC_BOUNCEBACK
+    p.wall_phi_mode = 1
+    p.force[0], p.force[2] = 1e-5, -1e-5
+    gpu, _ = run_gpu(p, f, 60)
+    o64, _ = run_oracle(p, f, 60, fp64=True)
+    o32, _ = run_oracle(p, f, 60, fp64=False)
+    assert_parity(gpu, o64, o32, "colour box")
