@@ -265,10 +265,15 @@ int launch_step(tslb_ctx* c) {
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
     dim3 block(TX, TY, 1);
     dim3 grid((c->nx + TX - 1) / TX, (c->ny + TY - 1) / TY, (c->nz + c->zchunk - 1) / c->zchunk);
-    if (c->p.mode == TSLB_MODE_COLOUR)
-        step_kernel<TSLB_MODE_COLOUR><<<grid, block, step_smem_bytes(TSLB_MODE_COLOUR), c->stream>>>(a);
-    else
-        step_kernel<TSLB_MODE_PHASEFIELD><<<grid, block, step_smem_bytes(TSLB_MODE_PHASEFIELD), c->stream>>>(a);
+    const bool vec = c->nx % 4 == 0;
+    const size_t sm = step_smem_bytes(c->p.mode);
+    if (c->p.mode == TSLB_MODE_COLOUR) {
+        if (vec) step_kernel<TSLB_MODE_COLOUR, true><<<grid, block, sm, c->stream>>>(a);
+        else step_kernel<TSLB_MODE_COLOUR, false><<<grid, block, sm, c->stream>>>(a);
+    } else {
+        if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true><<<grid, block, sm, c->stream>>>(a);
+        else step_kernel<TSLB_MODE_PHASEFIELD, false><<<grid, block, sm, c->stream>>>(a);
+    }
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
@@ -327,12 +332,15 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
         if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
     }
-    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)step_smem_bytes(TSLB_MODE_COLOUR))) != cudaSuccess)
-        return bail(e, "cudaFuncSetAttribute");
-    if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)step_smem_bytes(TSLB_MODE_PHASEFIELD))) != cudaSuccess)
-        return bail(e, "cudaFuncSetAttribute");
+    {
+        const int sc = (int)step_smem_bytes(TSLB_MODE_COLOUR), sp = (int)step_smem_bytes(TSLB_MODE_PHASEFIELD);
+        const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true>, attr, sc)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false>, attr, sc)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true>, attr, sp)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false>, attr, sp)) != cudaSuccess)
+            return bail(e, "cudaFuncSetAttribute");
+    }
     // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);

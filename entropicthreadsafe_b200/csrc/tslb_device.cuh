@@ -79,7 +79,11 @@ struct StepArgs {
 __device__ __forceinline__ long long nidx(const StepArgs& a, int x, int y, int z) {
     return (long long)x + (long long)a.nx * ((long long)y + (long long)a.ny * z);
 }
-__device__ __forceinline__ int wrapi(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+// periodic wrap of any coordinate into [0, n) (tiles may reach several periods out on tiny lattices)
+__device__ __forceinline__ int wrapi(int c, int n) {
+    c %= n;
+    return c < 0 ? c + n : c;
+}
 __device__ __forceinline__ int dimn(const StepArgs& a, int ax) { return ax == 0 ? a.nx : ax == 1 ? a.ny : a.nz; }
 
 __device__ __forceinline__ long long plane_index(const StepArgs& a, int face, int x, int y, int z) {

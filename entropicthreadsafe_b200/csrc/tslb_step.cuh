@@ -3,9 +3,12 @@
 // One CUDA block owns a TX x TY tile of (x, y) columns and a chunk of
 // `zchunk` target planes.  It marches through the source planes
 // s = z0-1 .. z1 of the chunk; for each:
+//   0. the moments of plane s+1 and phi of plane s+2 are copied into shared
+//      memory with cp.async (16-byte chunks when nx % 4 == 0), overlapping
+//      the work on plane s;
 //   1. every thread computes the coefficients of P'(c) (tslb_device.cuh) of
-//      some nodes of plane s (tile plus a one-node halo) into shared memory
-//      (double buffered, one __syncthreads per plane);
+//      one or two nodes of plane s (the tile plus a one-node rim) into
+//      shared memory (double buffered);
 //   2. every thread pulls, for its own column, the 27 populations that
 //      leave the 9 source nodes (x-ox, y-oy, s) and land on targets
 //      (x, y, s-1), (x, y, s), (x, y, s+1), accumulating the targets'
@@ -23,27 +26,37 @@
 
 namespace tslb {
 
-// P'(c) of one source node for the directions (CXv, CYv, cz), cz = -1, 0, 1:
-// P' = Q0 + cz Q1 + cz^2 Q2 with the node's coefficients at Kp (stride CAREA).
-template <int CXv, int CYv>
-__device__ __forceinline__ void eval_lateral(const float* __restrict__ Kp, float& Pm, float& P0, float& Pp) {
-    auto L = [&](int slot) { return Kp[slot * CAREA]; };
-    float q0 = L(K_0);
-    if (CXv) q0 += CXv * L(K_X) + L(K_XX);
-    if (CYv) q0 += CYv * L(K_Y) + L(K_YY);
-    if (CXv && CYv) q0 += (CXv * CYv) * L(K_XY) + CYv * L(K_XXY) + CXv * L(K_XYY);
-    float q1 = L(K_Z);
-    if (CXv) q1 += CXv * L(K_XZ) + L(K_XXZ);
-    if (CYv) q1 += CYv * L(K_YZ) + L(K_YYZ);
-    if (CXv && CYv) q1 += (CXv * CYv) * L(K_XYZ);
-    float q2 = L(K_ZZ);
-    if (CXv) q2 += CXv * L(K_XZZ);
-    if (CYv) q2 += CYv * L(K_YZZ);
-    const float t = q0 + q2;
-    Pm = t - q1;
-    P0 = q0;
-    Pp = t + q1;
+// Coefficients live in shared memory as NCOEF scalar planes of CAREA floats
+// (slot-major), so each source loads exactly the slots its directions use.
+__device__ __forceinline__ void store_coefs(float* dst, const float* K) {
+#pragma unroll
+    for (int c = 0; c < NCOEF; ++c) dst[c * CAREA] = K[c];
 }
+
+// P' = Q0 + cz Q1 + cz^2 Q2 of the directions (CXv, CYv, cz), cz = -1, 0, 1,
+// of the source whose coefficients start at Kp
+template <int CXv, int CYv>
+struct Src {
+    const float* Kp;
+    __device__ __forceinline__ float L(int slot) const { return Kp[slot * CAREA]; }
+    __device__ __forceinline__ void eval(float& Pm, float& P0, float& Pp) const {
+        float q0 = L(K_0);
+        if (CXv) q0 += CXv * L(K_X) + L(K_XX);
+        if (CYv) q0 += CYv * L(K_Y) + L(K_YY);
+        if (CXv && CYv) q0 += (CXv * CYv) * L(K_XY) + CYv * L(K_XXY) + CXv * L(K_XYY);
+        float q1 = L(K_Z);
+        if (CXv) q1 += CXv * L(K_XZ) + L(K_XXZ);
+        if (CYv) q1 += CYv * L(K_YZ) + L(K_YYZ);
+        if (CXv && CYv) q1 += (CXv * CYv) * L(K_XYZ);
+        float q2 = L(K_ZZ);
+        if (CXv) q2 += CXv * L(K_XZZ);
+        if (CYv) q2 += CYv * L(K_YZZ);
+        const float t = q0 + q2;
+        Pm = t - q1;
+        P0 = q0;
+        Pp = t + q1;
+    }
+};
 
 __host__ __device__ constexpr float w1d(int c) { return c == 0 ? 2.0f / 3.0f : 1.0f / 6.0f; }
 
@@ -86,28 +99,29 @@ __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float 
 
 // All populations that leave the source row y - CYv of plane s and land on
 // the column's targets in planes s-1 (accm), s (acc0), s+1 (accp).  Kc
-// points at the column's own node in the coefficient tile.
+// points at the column's own node in the coefficient tile; phm, ph0, php
+// are the column's own phi in the three target planes (colour mode).
 template <int MODE, int CYv>
 __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp,
                                          float phm, float ph0, float php) {
-    const float* Ka = Kc - CYv * CW - 1;  // source of cx = +1 (x - 1)
-    const float* Kz = Kc - CYv * CW;      // source of cx = 0
-    const float* Kb = Kc - CYv * CW + 1;  // source of cx = -1 (x + 1)
+    const Src<1, CYv> sa{Kc - CYv * CW - 1};   // source of cx = +1 (x - 1)
+    const Src<0, CYv> sz{Kc - CYv * CW};       // source of cx = 0
+    const Src<-1, CYv> sb{Kc - CYv * CW + 1};  // source of cx = -1 (x + 1)
     float am, a0, ap, cm, c0, cp, bm, b0, bp;
-    eval_lateral<1, CYv>(Ka, am, a0, ap);
-    eval_lateral<0, CYv>(Kz, cm, c0, cp);
-    eval_lateral<-1, CYv>(Kb, bm, b0, bp);
+    sa.eval(am, a0, ap);
+    sz.eval(cm, c0, cp);
+    sb.eval(bm, b0, bp);
     acc_group<CYv, -1>(accm, am, cm, bm);
     acc_group<CYv, 0>(acc0, a0, c0, b0);
     acc_group<CYv, 1>(accp, ap, cp, bp);
     if (MODE == TSLB_MODE_COLOUR) {
-        const float pa = Ka[K_C0 * CAREA], pz = Kz[K_C0 * CAREA], pb = Kb[K_C0 * CAREA];
+        const float pa = sa.L(K_C0), pz = sz.L(K_C0), pb = sb.L(K_C0);
         // recolouring sums over the cx = +1 / -1 sources
-        const float Ex = Ka[K_C1 * CAREA] - Kb[K_C1 * CAREA];
-        const float Ey = CYv ? Ka[K_C2 * CAREA] + Kb[K_C2 * CAREA] : 0.f;
-        const float Ez = Ka[K_C3 * CAREA] + Kb[K_C3 * CAREA];
-        const float By0 = CYv ? Kz[K_C2 * CAREA] : 0.f;
-        const float Bz0 = Kz[K_C3 * CAREA];
+        const float Ex = sa.L(K_C1) - sb.L(K_C1);
+        const float Ey = CYv ? sa.L(K_C2) + sb.L(K_C2) : 0.f;
+        const float Ez = sa.L(K_C3) + sb.L(K_C3);
+        const float By0 = CYv ? sz.L(K_C2) : 0.f;
+        const float Bz0 = sz.L(K_C3);
         // (phi_s - phi_t)(1 + P') for the three sources and the three target planes
         auto h = [](float ps, float pt, float P) { const float d = ps - pt; return fmaf(d, P, d); };
         col_group<CYv, -1>(accm, h(pa, phm, am), h(pz, phm, cm), h(pb, phm, bm), Ex, Ey, Ez, By0, Bz0);
@@ -116,19 +130,19 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
         if (CYv == 0) {
             // rest population: f_0 += delta0 (perturbation with B_0 = -10/27); its
             // colour is the target's own, so it adds no colour increment
-            acc0[A_RHO] += Kz[K_C4 * CAREA];
+            acc0[A_RHO] += sz.L(K_C4);
         }
     } else {
         // phase field g (D3Q7): axis directions and the rest population
         if (CYv == 0) {
-            const float g0 = Kz[K_C0 * CAREA], gz = Kz[K_C3 * CAREA];
-            accm[A_COL] += g0 - gz;   // q = 6, (0,0,-1)
-            accp[A_COL] += g0 + gz;   // q = 5, (0,0,+1)
-            acc0[A_COL] += Ka[K_C0 * CAREA] + Ka[K_C1 * CAREA];   // q = 1 from x - 1
-            acc0[A_COL] += Kb[K_C0 * CAREA] - Kb[K_C1 * CAREA];   // q = 2 from x + 1
-            acc0[A_COL] = fmaf(2.f, g0, acc0[A_COL]);            // q = 0: p0g phi = 2 G0
+            const float g0 = sz.L(K_C0), gz = sz.L(K_C3);
+            accm[A_COL] += g0 - gz;                        // q = 6, (0,0,-1)
+            accp[A_COL] += g0 + gz;                        // q = 5, (0,0,+1)
+            acc0[A_COL] += sa.L(K_C0) + sa.L(K_C1);        // q = 1 from x - 1
+            acc0[A_COL] += sb.L(K_C0) - sb.L(K_C1);        // q = 2 from x + 1
+            acc0[A_COL] = fmaf(2.f, g0, acc0[A_COL]);      // q = 0: p0g phi = 2 G0
         } else {
-            acc0[A_COL] += Kz[K_C0 * CAREA] + CYv * Kz[K_C2 * CAREA];  // q = 3 / 4
+            acc0[A_COL] += sz.L(K_C0) + CYv * sz.L(K_C2);  // q = 3 / 4
         }
     }
 }
@@ -136,9 +150,13 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 // Regularized or bounce-back populations entering target (x,y,z) from
 // behind non-periodic faces; Kp points at the target's own coefficients.
 template <int MODE>
-__device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp, unsigned mask, int x, int y, int z, float* acc) {
+__device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y, int z,
+                                float* acc) {
+    float Kp[NCOEF];
+#pragma unroll
+    for (int c = 0; c < NCOEF; ++c) Kp[c] = Kc[c * CAREA];
     // colour mode accumulates colour increments over the target's own phi
-    const float pht = Kp[K_C0 * CAREA];
+    const float pht = Kp[K_C0];
     // own raw moments (velocity faces only)
     float m[NF];
     bool have_m = false;
@@ -174,15 +192,15 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
         }
         if (vface < 0) {
             // half-way bounce-back: f_c(x) = f^post_{-c}(x)
-            const float P = eval_P(Kp, CAREA, -dx, -dy, -dz);
+            const float P = eval_P(Kp, 1, -dx, -dy, -dz);
             acc_dir_rt(acc, dx, dy, dz, wq * P);
             if (MODE == TSLB_MODE_COLOUR) {
                 // the reflected population carries the target's own colour: only the recolouring term
-                const float bc = -(dx * Kp[K_C1 * CAREA] + dy * Kp[K_C2 * CAREA] + dz * Kp[K_C3 * CAREA]);
+                const float bc = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
                 acc[A_COL] += wq * invlen(c2) * bc;
             } else if (c2 == 1) {
-                const float ge = -(dx * Kp[K_C1 * CAREA] + dy * Kp[K_C2 * CAREA] + dz * Kp[K_C3 * CAREA]);
-                acc[A_COL] += Kp[K_C0 * CAREA] + ge;
+                const float ge = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
+                acc[A_COL] += Kp[K_C0] + ge;
             }
         } else {
             if (!have_m) {
@@ -255,22 +273,32 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kp,
     }
 }
 
-// phi tile of a plane with a two-node halo (the gradient of the halo
-// coefficient nodes reaches two nodes out)
-constexpr int PW = TX + 4, PH = TY + 4, PAREA = PW * PH;
+// ---- shared-memory staging geometry ----
+// Moments and phi are staged with the tile's x range widened to 16-byte
+// chunks: columns x0-4 .. x0+TX+3 (SW = TX + 8 floats per row).
+constexpr int SW = TX + 8;
+constexpr int NCH = SW / 4;                   // 16-byte chunks per row
+constexpr int MROWS = CH;                     // moment rows: y0-1 .. y0+TY
+constexpr int PROWS = TY + 4;                 // phi rows: y0-2 .. y0+TY+1
+constexpr int MAREA = MROWS * SW, PAREA = PROWS * SW;
 constexpr int NTHR = TX * TY;
-constexpr int NHALO = CAREA - NTHR;          // coefficient nodes on the tile rim (84)
-constexpr int NPHI_ROUNDS = (PAREA + NTHR - 1) / NTHR;
+constexpr int NHALO = CAREA - NTHR;           // coefficient nodes on the tile rim (84)
+constexpr int NMOM = NF - 1;                  // moments staged per node (phi comes from the phi ring)
+constexpr int MCOPIES = NMOM * MROWS * NCH;   // 16-byte copies of one moment plane
+constexpr int MROUNDS = (MCOPIES + NTHR - 1) / NTHR;
+constexpr int PCOPIES = PROWS * NCH;          // 16-byte copies of one phi plane
+constexpr int PELEMS = PROWS * SW;
+constexpr int PEROUNDS = (PELEMS + NTHR - 1) / NTHR;
 
 __host__ __device__ constexpr size_t step_smem_bytes(int mode) {
-    return sizeof(float) * (2 * NCOEF * CAREA + 2 * (NF - 1) * CAREA + (mode == TSLB_MODE_COLOUR ? 4 * PAREA : 0));
+    return sizeof(float) * 2 * NCOEF * CAREA + sizeof(float) * 2 * NMOM * MAREA +
+           (mode == TSLB_MODE_COLOUR ? sizeof(float) * 4 * PAREA : 0);
 }
 
 // gradient 3 sum_i p_i c_i phi(x+c_i) from three phi planes held in shared
-// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch PW)
+// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch SW)
 __device__ __forceinline__ void grad_smem(const float* pm, const float* p0, const float* pp, float g[3]) {
-    // x: +x face minus -x face, grouped by weight class
-    auto P = [&](const float* pl, int dx, int dy) { return pl[dy * PW + dx]; };
+    auto P = [&](const float* pl, int dx, int dy) { return pl[dy * SW + dx]; };
     const float x1 = P(p0, 1, 0) - P(p0, -1, 0);
     const float x2 = (P(p0, 1, 1) + P(p0, 1, -1) + P(pp, 1, 0) + P(pm, 1, 0)) -
                      (P(p0, -1, 1) + P(p0, -1, -1) + P(pp, -1, 0) + P(pm, -1, 0));
@@ -314,18 +342,21 @@ __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async16(float* sdst, const float* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-constexpr int NMOM = NF - 1;  // moments staged per coefficient node (phi comes from the phi ring)
-
-template <int MODE>
+// VEC: nx % 4 == 0, so 16-byte chunks of a row never straddle the x faces
+template <int MODE, bool VEC>
 __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
-    extern __shared__ float smem[];
-    float* coef_base = smem;                          // [2][NCOEF][CAREA]
-    float* mst = coef_base + 2 * NCOEF * CAREA;       // [2][NMOM][CAREA] staged moments
-    float* phis = mst + 2 * NMOM * CAREA;             // colour: [4][PAREA] ring of phi planes
+    extern __shared__ float4 smem4[];
+    float* coef_base = reinterpret_cast<float*>(smem4);   // [2][NCOEF][CAREA]
+    float* mst = coef_base + 2 * NCOEF * CAREA;           // [2][NMOM][MROWS][SW]
+    float* phis = mst + 2 * NMOM * MAREA;                             // colour: [4][PROWS][SW]
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * a.zchunk;
@@ -346,69 +377,112 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         if (!yper && Y == a.ny - 1) colmask |= 8u;
     }
 
-    // coefficient nodes of this thread: its own column, and one rim node
-    XYNode cn[2];
-    int cidx[2];
-    cn[0] = xy_node(a, X, Y, xper, yper);
-    cidx[0] = (ty + 1) * CW + (tx + 1);
+    // coefficient nodes of this thread: its own column (r = 0) and one rim node (r = 1)
     const bool has_rim = tid < NHALO;
+    XYNode cn0 = xy_node(a, X, Y, xper, yper), cn1;
+    const int ci0 = (ty + 1) * CW + (tx + 1);
+    int ci1;
     {
         int h = has_rim ? tid : 0, cx, cy;
         if (h < CW) { cx = h; cy = 0; }
         else if (h < 2 * CW) { cx = h - CW; cy = CH - 1; }
         else if (h < 2 * CW + TY) { cx = 0; cy = h - 2 * CW + 1; }
         else { cx = CW - 1; cy = h - 2 * CW - TY + 1; }
-        cn[1] = xy_node(a, x0 - 1 + cx, y0 - 1 + cy, xper, yper);
-        cidx[1] = cy * CW + cx;
+        cn1 = xy_node(a, x0 - 1 + cx, y0 - 1 + cy, xper, yper);
+        ci1 = cy * CW + cx;
     }
+    // position of a coefficient node (cx, cy) in the staged planes: moments
+    // row cy, column cx + 3; phi row cy + 1, column cx + 3
+    const int mi0 = (ci0 / CW) * SW + (ci0 % CW) + 3, mi1 = (ci1 / CW) * SW + (ci1 % CW) + 3;
+    const int pi0 = mi0 + SW, pi1 = mi1 + SW;
     const int nnodes = has_rim ? 2 : 1;
-    int pidx[2];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) pidx[r] = (cidx[r] / CW + 1) * PW + (cidx[r] % CW + 1);
-    // phi nodes this thread stages (colour mode)
-    XYNode pn[NPHI_ROUNDS];
-#pragma unroll
-    for (int r = 0; r < NPHI_ROUNDS; ++r) {
-        int j = tid + r * NTHR;
-        j = j < PAREA ? j : 0;
-        pn[r] = xy_node(a, x0 - 2 + j % PW, y0 - 2 + j / PW, xper, yper);
-    }
 
     auto zwrap = [&](int z, bool& out) {
         out = false;
         if (z < 0 || z >= a.nz) { if (zper) return wrapi(z, a.nz); out = true; }
         return z;
     };
-    // stage phi of plane z into ring slot z & 3 (asynchronous copies, ghost
-    // values computed)
+
+    // ---- staging of phi planes (colour mode) ----
+    // VEC: copy j < PCOPIES is the 16-byte chunk (row j / NCH, chunk j % NCH);
+    // a chunk is either fully inside the domain (after the periodic wrap) or
+    // fully behind a non-periodic face, whose ghost values are computed.
+    int pch_off = 0;
+    bool pch_out = true;
+    if (VEC && tid < PCOPIES) {
+        const int row = tid / NCH, ch = tid % NCH;
+        const XYNode nd = xy_node(a, x0 - 4 + 4 * ch, y0 - 2 + row, xper, yper);
+        pch_off = nd.off;
+        pch_out = nd.out;
+    }
     auto stage_phi = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
         float* slot = phis + (z & 3) * PAREA;
         const float* ph = a.in + F_PHI * a.N + (long long)gz * plane;
+        if (VEC) {
+            if (tid < PCOPIES) {
+                const int row = tid / NCH, ch = tid % NCH;
+                float* dst = slot + row * SW + 4 * ch;
+                if (!pch_out && !zout) {
+                    cp_async16(dst, ph + pch_off);
+                } else {
 #pragma unroll
-        for (int r = 0; r < NPHI_ROUNDS; ++r) {
-            const int j = tid + r * NTHR;
-            if (j < PAREA) {
-                if (!pn[r].out && !zout) cp_async4(slot + j, ph + pn[r].off);
-                else slot[j] = phi_at(a, pn[r].gx, pn[r].gy, z);
+                    for (int e = 0; e < 4; ++e) dst[e] = phi_at(a, x0 - 4 + 4 * ch + e, y0 - 2 + row, z);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < PEROUNDS; ++r) {
+                const int j = tid + r * NTHR;
+                if (j < PELEMS) {
+                    const int row = j / SW, col = j % SW;
+                    const XYNode nd = xy_node(a, x0 - 4 + col, y0 - 2 + row, xper, yper);
+                    if (!nd.out && !zout) cp_async4(slot + j, ph + nd.off);
+                    else slot[j] = phi_at(a, nd.gx, nd.gy, z);
+                }
             }
         }
     };
-    // stage the 10 non-phi moments of this thread's coefficient nodes of plane z
+
+    // ---- staging of the 10 non-phi moments of plane z ----
+    // VEC: copy j = tid + r NTHR < MCOPIES is (field j / (MROWS NCH), row, chunk)
+    int mch_off[MROUNDS];
+    unsigned mch_ok = 0;
+    if (VEC) {
+#pragma unroll
+        for (int r = 0; r < MROUNDS; ++r) {
+            const int j = tid + r * NTHR;
+            const int rem = j % (MROWS * NCH), row = rem / NCH, ch = rem % NCH;
+            const XYNode nd = xy_node(a, x0 - 4 + 4 * ch, y0 - 1 + row, xper, yper);
+            mch_off[r] = nd.off;
+            if (j < MCOPIES && !nd.out) mch_ok |= 1u << r;
+        }
+    }
     auto stage_mom = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
         if (zout) return;
-        float* dst = mst + (z & 1) * (NMOM * CAREA);
+        float* dst = mst + (z & 1) * (NMOM * MAREA);
         const float* src = a.in + (long long)gz * plane;
-        for (int r = 0; r < nnodes; ++r) {
-            const XYNode nd = r ? cn[1] : cn[0];
-            if (nd.out) continue;
-            const float* p = src + nd.off;
-            float* d = dst + (r ? cidx[1] : cidx[0]);
+        if (VEC) {
 #pragma unroll
-            for (int f = 0; f < NMOM; ++f) cp_async4(d + f * CAREA, p + f * a.N);
+            for (int r = 0; r < MROUNDS; ++r) {
+                if (!(mch_ok & (1u << r))) continue;
+                const int j = tid + r * NTHR;
+                const int f = j / (MROWS * NCH), rem = j % (MROWS * NCH);
+                const int row = rem / NCH, ch = rem % NCH;
+                cp_async16(dst + f * MAREA + row * SW + 4 * ch, src + f * a.N + mch_off[r]);
+            }
+        } else {
+            for (int r = 0; r < nnodes; ++r) {
+                const XYNode nd = r ? cn1 : cn0;
+                if (nd.out) continue;
+                const float* p = src + nd.off;
+                float* d = dst + (r ? mi1 : mi0);
+#pragma unroll
+                for (int f = 0; f < NMOM; ++f) cp_async4(d + f * MAREA, p + f * a.N);
+            }
         }
     };
 
@@ -435,16 +509,18 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         cp_async_commit();
         if (more) stage_mom(s + 1);
         cp_async_commit();
-        cp_async_wait<2>();  // this thread's moments of plane s have landed
+        cp_async_wait<2>();  // this thread's moment copies of plane s have landed
+        // VEC staging lets any thread copy any node's moments: make them visible
+        if (VEC) __syncthreads();
         // ---- 1. coefficients of source plane s: own column and one rim node ----
         bool zsolid;
         const int gz = zwrap(s, zsolid);
-        const float* ms = mst + (s & 1) * (NMOM * CAREA);
+        const float* ms = mst + (s & 1) * (NMOM * MAREA);
         // a solid source plane sends nothing: no coefficients, no pull
         for (int r = 0; r < (zsolid ? 0 : nnodes); ++r) {
-            const XYNode nd = r ? cn[1] : cn[0];
-            const int ci = r ? cidx[1] : cidx[0];
-            const int pi = r ? pidx[1] : pidx[0];
+            const XYNode nd = r ? cn1 : cn0;
+            const int ci = r ? ci1 : ci0;
+            const int mi = r ? mi1 : mi0;
             float K[NCOEF];
             if (nd.out) {
 #pragma unroll
@@ -452,9 +528,11 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
             } else {
                 float m[NF];
 #pragma unroll
-                for (int f = 0; f < NMOM; ++f) m[f] = ms[f * CAREA + ci];
+                for (int f = 0; f < NMOM; ++f) m[f] = ms[f * MAREA + mi];
                 float g[3] = {0.f, 0.f, 0.f};
+                int gx = 0, gy = 0;
                 if (MODE == TSLB_MODE_COLOUR) {
+                    const int pi = r ? pi1 : pi0;
                     const float* p0 = phis + (s & 3) * PAREA + pi;
                     const float* pm = phis + ((s - 1) & 3) * PAREA + pi;
                     const float* pp = phis + ((s + 1) & 3) * PAREA + pi;
@@ -462,13 +540,12 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
                     grad_smem(pm, p0, pp, g);
                 } else {
                     m[F_PHI] = __ldg(a.in + F_PHI * a.N + (long long)gz * plane + nd.off);
+                    gx = nd.off % a.nx;
+                    gy = nd.off / a.nx;
                 }
-                const int gx = nd.off % a.nx, gy = nd.off / a.nx;
                 node_coefs<MODE>(a, m, g, gx, gy, gz, K);
             }
-            float* dst = coef + ci;
-#pragma unroll
-            for (int c = 0; c < NCOEF; ++c) dst[c * CAREA] = K[c];
+            store_coefs(coef + ci, K);
         }
         cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
@@ -478,7 +555,7 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
                 // own-column phi of the target planes (the ring holds planes s-1 .. s+2)
-                const int po = (ty + 2) * PW + (tx + 2);
+                const int po = (ty + 2) * SW + (tx + 4);
                 phm = phis[((s - 1) & 3) * PAREA + po];
                 ph0 = phis[(s & 3) * PAREA + po];
                 php = phis[((s + 1) & 3) * PAREA + po];
@@ -512,7 +589,7 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
                 o[F_YZ] = accm[A_YZ] - rho * v * w;
                 // colour mode: phi_t + (colour increment) / rho
                 o[F_PHI] = MODE == TSLB_MODE_COLOUR ? fmaf(accm[A_COL], inv, phm) : accm[A_COL];
-                float* po = a.out + (long long)t * plane + cn[0].off;
+                float* po = a.out + (long long)t * plane + cn0.off;
                 float chk = 0.f;
 #pragma unroll
                 for (int f = 0; f < NF; ++f) {
