@@ -20,6 +20,7 @@ PREC_FP32, PREC_BF16, PREC_FP16S = 0, 1, 2
 BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET = range(5)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
 NREDUCE = 12
+NOALLOC_MAX_NODES = 1 << 20
 RED_NAMES = ("mass", "mass_a", "mass_b", "mom_x", "mom_y", "mom_z", "kinetic",
              "umax", "rho_in", "rho_out", "dp", "n_in")
 FIELDS = ("rho", "u", "v", "w", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "phi")
@@ -127,6 +128,8 @@ def lib() -> ctypes.CDLL:
         L.tslb_launch_count.restype = ctypes.c_longlong
         L.tslb_last_error.argtypes = [vp]
         L.tslb_last_error.restype = ctypes.c_char_p
+        L.tslb_step_noalloc.argtypes = [vp, ip, ip, ip, vp, vp, ctypes.c_longlong, vp]
+        L.tslb_step_noalloc.restype = ip
         _lib = L
     return _lib
 

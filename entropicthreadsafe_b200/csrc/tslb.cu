@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -503,3 +504,112 @@ const char* tslb_last_error(tslb_ctx* c) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- step without allocation
+// Scratch of tslb_step_noalloc: a fixed device array of this file.  In host
+// code these names are host-side stand-ins, not device addresses; the
+// addresses come from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) float g_noalloc_normals[3 * TSLB_NOALLOC_MAX_NODES];
+static __device__ __align__(256) unsigned int g_noalloc_flags[64];
+
+namespace {
+constexpr int kMaxDevices = 64;
+struct NoallocScratch {
+    bool ready = false;
+    float* normals = nullptr;
+    unsigned int* flags = nullptr;
+};
+NoallocScratch g_noalloc[kMaxDevices];
+std::mutex g_noalloc_mu;
+
+// context-free failures report through tslb_last_error(NULL)
+int noalloc_fail(int code, const std::string& msg) {
+    g_create_error = msg;
+    return code;
+}
+
+// Once per device, with that device current: resolve the scratch address
+// and set the step kernels' shared-memory attribute.
+int noalloc_setup(int dev, NoallocScratch** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoallocScratch& s = g_noalloc[dev];
+    if (!s.ready) {
+        cudaError_t e = cudaGetSymbolAddress((void**)&s.normals, g_noalloc_normals);
+        if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(normals): ") + cudaGetErrorString(e));
+        e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
+        if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(flags): ") + cudaGetErrorString(e));
+        const int sc = (int)step_smem_bytes(TSLB_MODE_COLOUR), sp = (int)step_smem_bytes(TSLB_MODE_PHASEFIELD);
+        const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true>, attr, sc)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false>, attr, sc)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true>, attr, sp)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false>, attr, sp)) != cudaSuccess)
+            return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        s.ready = true;
+    }
+    *out = &s;
+    return TSLB_OK;
+}
+}  // namespace
+
+extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, const float* d_in, float* d_out,
+                                 long long field_stride, void* stream) {
+    std::string why;
+    int rc = validate(p, nx, ny, nz, why);
+    if (rc) return noalloc_fail(rc, "tslb_step_noalloc: " + why);
+    const long long n = (long long)nx * ny * nz;
+    if (n > TSLB_NOALLOC_MAX_NODES)
+        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: " + std::to_string(n) + " nodes exceed the scratch limit of " +
+                                              std::to_string(TSLB_NOALLOC_MAX_NODES) + " (TSLB_NOALLOC_MAX_NODES)");
+    if (!d_in || !d_out || d_in == d_out) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be distinct device buffers");
+    if (field_stride < n || field_stride % 4 != 0)
+        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: field_stride must be >= nx*ny*nz and a multiple of 4");
+    if (((uintptr_t)d_in | (uintptr_t)d_out) % 16 != 0)
+        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be 16-byte aligned");
+    for (int f = 0; f < 6; ++f)
+        if (p->bc[f] == TSLB_BC_INLET) return noalloc_fail(TSLB_ERR_UNSUPPORTED, "tslb_step_noalloc: inlet faces are not supported");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: device ordinal out of range");
+    NoallocScratch* sc = nullptr;
+    rc = noalloc_setup(dev, &sc);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the flag starts at zero on every call
+    e = cudaMemsetAsync(sc->flags, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    // a context-free view of the lattice for make_args
+    tslb_ctx view;
+    view.p = *p;
+    view.nx = nx; view.ny = ny; view.nz = nz;
+    view.n = n; view.N = field_stride;
+    view.nrm = sc->normals;
+    view.flags = sc->flags;
+    view.stream = st;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+    const long long want = 8LL * sms;
+    view.zchunk = (int)std::min<long long>(nz, std::max<long long>(8, (tiles * nz + want - 1) / want));
+    if (p->mode == TSLB_MODE_PHASEFIELD) {
+        StepArgs an = make_args(&view, d_in, nullptr);
+        const int bs = 256;
+        normals_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(an, sc->normals);
+        if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("normals launch: ") + cudaGetErrorString(e));
+    }
+    StepArgs a = make_args(&view, d_in, d_out);
+    dim3 block(TX, TY, 1);
+    dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (nz + view.zchunk - 1) / view.zchunk);
+    const bool vec = nx % 4 == 0;
+    const size_t sm = step_smem_bytes(p->mode);
+    if (p->mode == TSLB_MODE_COLOUR) {
+        if (vec) step_kernel<TSLB_MODE_COLOUR, true><<<grid, block, sm, st>>>(a);
+        else step_kernel<TSLB_MODE_COLOUR, false><<<grid, block, sm, st>>>(a);
+    } else {
+        if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true><<<grid, block, sm, st>>>(a);
+        else step_kernel<TSLB_MODE_PHASEFIELD, false><<<grid, block, sm, st>>>(a);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+    return TSLB_OK;
+}

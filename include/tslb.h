@@ -174,9 +174,38 @@ void* tslb_stream(tslb_ctx* ctx);
 /* Number of kernel launches the context has issued since creation. */
 long long tslb_launch_count(tslb_ctx* ctx);
 
-/* Message of the last failed call on ctx (or of the last failed
- * tslb_create when ctx is NULL).  Never NULL. */
+/* Message of the last failed call on ctx (or, when ctx is NULL, of the
+ * last failed tslb_create or tslb_step_noalloc).  Never NULL. */
 const char* tslb_last_error(tslb_ctx* ctx);
+
+/* Largest lattice (nodes) tslb_step_noalloc accepts. */
+#define TSLB_NOALLOC_MAX_NODES (1LL << 20)
+
+/* One time step on caller-owned device buffers, allocating nothing.
+ *
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- a host that owns all device memory itself (an OpenACC data
+ * region, a memory pool, a real-time loop that must not allocate).  The
+ * scratch the step needs (interface normals of the phase-field mode, the
+ * non-finite flag) lives in a fixed device array inside the library, sized
+ * for TSLB_NOALLOC_MAX_NODES nodes (12 MB on every GPU that loads the
+ * library, held until the process exits); larger lattices are rejected.
+ *
+ * d_in and d_out hold the 11 fields in the library's device layout: field
+ * f at d_x + f * field_stride (floats), x fastest, field 0 = rho - 1, then
+ * u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi.  Both 16-byte aligned,
+ * field_stride >= nx*ny*nz and a multiple of 4, d_in != d_out.  Inlet
+ * faces are not supported (their planes need storage).  The work is queued
+ * on `stream` (cudaStream_t, NULL = default stream) and not waited for; no
+ * non-finite check is reported.
+ *
+ * The first call on a device resolves the scratch address and sets kernel
+ * attributes; make that first call before any stream capture.  All calls
+ * share the one scratch array, so calls that overlap on the GPU (other
+ * streams, other threads) race: order them on one stream. */
+int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz,
+                      const float* d_in, float* d_out, long long field_stride,
+                      void* stream);
 
 #ifdef __cplusplus
 }
