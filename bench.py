@@ -267,8 +267,33 @@ def run_ours(args):
         ms_max = float(t.item())
     value = ws * nodes * args.steps / (ms_max * 1e-3) / 1e6
     ms_step = ms_max / args.steps
+    # ---- precision forms of the same workload (bf16, fp16 with per-field scale) ----
+    forms = None
+    if not args.no_precision_forms:
+        forms = {}
+        lat.close()
+        for name, prec in (("bf16", capi.PREC_BF16), ("fp16s", capi.PREC_FP16S)):
+            p.precision = prec
+            lp = Lattice(p, nx, ny, nz)
+            sp = torch.cuda.ExternalStream(lp.stream)
+            lp.upload_moments(f)
+            lp.step(args.warmup)
+            lp.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(sp)
+            lp.step(args.steps)
+            e1.record(sp)
+            lp.synchronize()
+            ms_p = e0.elapsed_time(e1) / args.steps
+            forms[name] = {"value": ws * nodes / (ms_p * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_p,
+                           "speedup_vs_fp32": ms_step / ms_p, "bytes_per_lu": 44}
+            lp.close()
+        p.precision = capi.PREC_FP32
+        lat = None
     # ---- end to end through the public API with host buffers ----
-    lat.close()
+    if lat is not None:
+        lat.close()
     barrier_sync()
     e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     state_bytes = 11 * 4 * nodes
@@ -294,6 +319,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}", "l2": "state 830 MB > 126 MB L2, no flush needed",
                    "state_bytes": state_bytes},
         "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+        "precision_forms": forms,
         "clocks": clk, "check": {"mass": red["mass"], "umax": red["umax"], "mass_a": red["mass_a"]},
     }
     print(json.dumps(line), flush=True)
@@ -311,6 +337,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-precision-forms", action="store_true", help="skip the bf16 / fp16 storage legs")
     ap.add_argument("--nz", type=int, default=0, help="shallower channel (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -23,7 +23,10 @@ struct tslb_ctx {
     long long N;        // padded field stride
     int device;
     cudaStream_t stream = nullptr;
-    float* state[2] = {nullptr, nullptr};  // ping-pong, 11 fields each
+    void* state[2] = {nullptr, nullptr};   // ping-pong, 11 fields each, storage type
+    int esize = 4;                         // bytes per stored element
+    float* io = nullptr;                   // FP32 conversion buffer (bf16/fp16 storage)
+    float scale[NF];                       // fp16 storage: stored = value * scale
     int cur = 0;
     float* nrm = nullptr;                  // 3 fields
     float* inlet[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -62,7 +65,9 @@ int validate(const tslb_params* p, int nx, int ny, int nz, std::string& why) {
     if (nx < 1 || ny < 1 || nz < 1) { why = "sizes must be >= 1"; return TSLB_ERR_ARG; }
     if ((long long)nx * ny * nz > (1LL << 36)) { why = "lattice too large"; return TSLB_ERR_ARG; }
     if (p->mode != TSLB_MODE_PHASEFIELD && p->mode != TSLB_MODE_COLOUR) { why = "unknown mode"; return TSLB_ERR_ARG; }
-    if (p->precision != TSLB_PREC_FP32) { why = "only TSLB_PREC_FP32 storage is implemented"; return TSLB_ERR_UNSUPPORTED; }
+    if (p->precision != TSLB_PREC_FP32 && p->precision != TSLB_PREC_BF16 && p->precision != TSLB_PREC_FP16S) {
+        why = "unknown precision"; return TSLB_ERR_ARG;
+    }
     if (!(p->tau_a > 0.5f) || !std::isfinite(p->tau_a)) { why = "tau_a must be > 0.5"; return TSLB_ERR_ARG; }
     if (p->mode == TSLB_MODE_COLOUR && (!(p->tau_b > 0.5f) || !std::isfinite(p->tau_b))) { why = "tau_b must be > 0.5"; return TSLB_ERR_ARG; }
     if (!std::isfinite(p->sigma) || !std::isfinite(p->beta) || !std::isfinite(p->sharp_c) || !std::isfinite(p->grad_threshold)) {
@@ -83,7 +88,7 @@ int validate(const tslb_params* p, int nx, int ny, int nz, std::string& why) {
     return TSLB_OK;
 }
 
-StepArgs make_args(tslb_ctx* c, const float* in, float* out) {
+StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
     StepArgs a;
     std::memset(&a, 0, sizeof(a));
     a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = c->N;
@@ -104,17 +109,22 @@ StepArgs make_args(tslb_ctx* c, const float* in, float* out) {
         a.face[f].plane = c->inlet[f];
     }
     a.flags = c->flags;
+    for (int f = 0; f < NF; ++f) {
+        a.scale[f] = c->scale[f];
+        a.iscale[f] = 1.0f / c->scale[f];
+    }
     return a;
 }
 
 // ---------------------------------------------------------------- kernels
+template <class T>
 __global__ void normals_kernel(const StepArgs a, float* nrm) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long n = (long long)a.nx * a.ny * a.nz;
     if (i >= n) return;
     const int x = (int)(i % a.nx), y = (int)((i / a.nx) % a.ny), z = (int)(i / ((long long)a.nx * a.ny));
     float g[3];
-    grad_phi(a, x, y, z, g);
+    grad_phi<T>(a, x, y, z, g);
     const float den = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + 1e-9f;
     nrm[i] = g[0] / den;
     nrm[a.N + i] = g[1] / den;
@@ -125,6 +135,23 @@ __global__ void normals_kernel(const StepArgs a, float* nrm) {
 __global__ void shift_rho_kernel(float* d, long long n) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) d[i] = d[i] - 1.0f;
+}
+
+// FP32 fields (rho already shifted to rho - 1) -> storage type
+template <class T>
+__global__ void to_storage_kernel(const float* __restrict__ src, T* __restrict__ dst, long long N, long long n, StepArgs a) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) dst[f * N + i] = cvt_out<T>(src[f * N + i], a, f);
+}
+// storage type -> FP32 fields (rho stays rho - 1)
+template <class T>
+__global__ void from_storage_kernel(const T* __restrict__ src, float* __restrict__ dst, long long N, long long n, StepArgs a) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) dst[f * N + i] = cvt_in<T>(src[f * N + i], a, f);
 }
 
 // Moments pass of the reference on populations in its halo layout
@@ -247,16 +274,64 @@ int check_flags(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+// Call fn with a value of the storage type of precision `prec`.
+template <class Fn>
+void with_storage(int prec, Fn&& fn) {
+    if (prec == TSLB_PREC_BF16) fn(__nv_bfloat16{});
+    else if (prec == TSLB_PREC_FP16S) fn(__half{});
+    else fn(float{});
+}
+
+int storage_bytes(int prec) { return prec == TSLB_PREC_FP32 ? 4 : 2; }
+
+// every step-kernel instantiation may use the opt-in shared memory it needs
+cudaError_t set_step_attributes() {
+    cudaError_t e = cudaSuccess;
+    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    auto one = [&](auto tag) {
+        using T = decltype(tag);
+        const int es = (int)sizeof(T);
+        const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, es), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, es);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, T>, attr, sc);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, T>, attr, sc);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true, T>, attr, sp);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false, T>, attr, sp);
+    };
+    one(float{});
+    one(__nv_bfloat16{});
+    one(__half{});
+    return e;
+}
+
 int launch_normals(tslb_ctx* c) {
     StepArgs a = make_args(c, c->state[c->cur], nullptr);
     const int bs = 256;
     const long long grid = (c->n + bs - 1) / bs;
-    normals_kernel<<<(unsigned)grid, bs, 0, c->stream>>>(a, c->nrm);
+    with_storage(c->p.precision, [&](auto tag) {
+        normals_kernel<decltype(tag)><<<(unsigned)grid, bs, 0, c->stream>>>(a, c->nrm);
+    });
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     return TSLB_OK;
 }
 
+// the step kernel on one lattice (shared by the context and the no-alloc paths)
+void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) {
+    dim3 block(TX, TY, 1);
+    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zchunk - 1) / a.zchunk);
+    with_storage(prec, [&](auto tag) {
+        using T = decltype(tag);
+        const bool vec = a.nx % (16 / (int)sizeof(T)) == 0;
+        const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
+        if (mode == TSLB_MODE_COLOUR) {
+            if (vec) step_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, st>>>(a);
+            else step_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, st>>>(a);
+        } else {
+            if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true, T><<<grid, block, sm, st>>>(a);
+            else step_kernel<TSLB_MODE_PHASEFIELD, false, T><<<grid, block, sm, st>>>(a);
+        }
+    });
+}
 
 int launch_step(tslb_ctx* c) {
     if (c->p.mode == TSLB_MODE_PHASEFIELD) {
@@ -264,21 +339,59 @@ int launch_step(tslb_ctx* c) {
         if (rc) return rc;
     }
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    dim3 block(TX, TY, 1);
-    dim3 grid((c->nx + TX - 1) / TX, (c->ny + TY - 1) / TY, (c->nz + c->zchunk - 1) / c->zchunk);
-    const bool vec = c->nx % 4 == 0;
-    const size_t sm = step_smem_bytes(c->p.mode);
-    if (c->p.mode == TSLB_MODE_COLOUR) {
-        if (vec) step_kernel<TSLB_MODE_COLOUR, true><<<grid, block, sm, c->stream>>>(a);
-        else step_kernel<TSLB_MODE_COLOUR, false><<<grid, block, sm, c->stream>>>(a);
-    } else {
-        if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true><<<grid, block, sm, c->stream>>>(a);
-        else step_kernel<TSLB_MODE_PHASEFIELD, false><<<grid, block, sm, c->stream>>>(a);
-    }
+    launch_step_kernel(a, c->p.mode, c->p.precision, c->stream);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
     return TSLB_OK;
+}
+
+// FP32 fields in io (rho already shifted) -> the state in its storage type
+int io_to_state(tslb_ctx* c) {
+    StepArgs a = make_args(c, nullptr, nullptr);
+    const int bs = 256;
+    with_storage(c->p.precision, [&](auto tag) {
+        using T = decltype(tag);
+        to_storage_kernel<T><<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(c->io, reinterpret_cast<T*>(c->state[c->cur]), c->N, c->n, a);
+    });
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
+// the state -> FP32 fields in io (rho stays rho - 1)
+int state_to_io(tslb_ctx* c) {
+    StepArgs a = make_args(c, nullptr, nullptr);
+    const int bs = 256;
+    with_storage(c->p.precision, [&](auto tag) {
+        using T = decltype(tag);
+        from_storage_kernel<T><<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(reinterpret_cast<const T*>(c->state[c->cur]), c->io, c->N, c->n, a);
+    });
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
+// FP32 view of the current state: the state itself, or io after conversion
+int fp32_view(tslb_ctx* c, const float** out) {
+    if (c->p.precision == TSLB_PREC_FP32) {
+        *out = static_cast<const float*>(c->state[c->cur]);
+        return TSLB_OK;
+    }
+    int rc = state_to_io(c);
+    *out = c->io;
+    return rc;
+}
+
+// Default power-of-two scales of fp16 storage: stored magnitudes near 2^10
+// for typical moments (|rho - 1| < 1/16, |u| < 1/4, |Pi^neq| < 1/16, |phi| <= 1).
+void default_scales(tslb_ctx* c) {
+    for (int f = 0; f < NF; ++f) c->scale[f] = 1.0f;
+    if (c->p.precision != TSLB_PREC_FP16S) return;
+    c->scale[F_D] = 16384.f;
+    c->scale[F_U] = c->scale[F_V] = c->scale[F_W] = 4096.f;
+    for (int f = F_XX; f <= F_ZZ; ++f) c->scale[f] = 16384.f;
+    c->scale[F_PHI] = 1024.f;
 }
 
 }  // namespace
@@ -321,8 +434,12 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     cudaError_t e;
     if ((e = cudaGetDevice(&c->device)) != cudaSuccess) return bail(e, "cudaGetDevice");
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "cudaStreamCreate");
+    c->esize = storage_bytes(p->precision);
+    default_scales(c);
     for (int b = 0; b < 2; ++b)
-        if ((e = cudaMalloc(&c->state[b], sizeof(float) * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+        if ((e = cudaMalloc(&c->state[b], (size_t)c->esize * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+    if (p->precision != TSLB_PREC_FP32)
+        if ((e = cudaMalloc(&c->io, sizeof(float) * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(io)");
     if ((e = cudaMalloc(&c->nrm, sizeof(float) * 3 * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(normals)");
     if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
     if ((e = cudaMalloc(&c->red, sizeof(double) * (RED_SLOTS + 1))) != cudaSuccess) return bail(e, "cudaMalloc(reduce)");
@@ -333,15 +450,7 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
         if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
     }
-    {
-        const int sc = (int)step_smem_bytes(TSLB_MODE_COLOUR), sp = (int)step_smem_bytes(TSLB_MODE_PHASEFIELD);
-        const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true>, attr, sc)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false>, attr, sc)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true>, attr, sp)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false>, attr, sp)) != cudaSuccess)
-            return bail(e, "cudaFuncSetAttribute");
-    }
+    if ((e = set_step_attributes()) != cudaSuccess) return bail(e, "cudaFuncSetAttribute");
     // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -357,6 +466,7 @@ void tslb_destroy(tslb_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int b = 0; b < 2; ++b) cudaFree(c->state[b]);
+    cudaFree(c->io);
     cudaFree(c->nrm);
     cudaFree(c->flags);
     cudaFree(c->red);
@@ -372,13 +482,33 @@ int tslb_upload_moments(tslb_ctx* c, const float* rho, const float* u, const flo
     const float* src[NF] = {rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi};
     for (int f = 0; f < NF; ++f)
         if (!src[f]) return fail(c, TSLB_ERR_ARG, "tslb_upload_moments: NULL field");
-    float* s = c->state[c->cur];
+    const bool fp32 = c->p.precision == TSLB_PREC_FP32;
+    float* s = fp32 ? static_cast<float*>(c->state[c->cur]) : c->io;
+    if (c->p.precision == TSLB_PREC_FP16S) {
+        // per-field power-of-two scales from the data: largest |value| near 2^10
+        default_scales(c);
+        for (int f = 0; f < NF; ++f) {
+            double mx = 0.0;
+            for (long long i = 0; i < c->n; ++i) {
+                const double v = f == F_D ? (double)src[f][i] - 1.0 : (double)src[f][i];
+                mx = std::max(mx, std::fabs(v));
+            }
+            if (mx > 0.0 && std::isfinite(mx)) {
+                const int k = std::max(-8, std::min(24, (int)std::floor(std::log2(1024.0 / mx))));
+                c->scale[f] = std::ldexp(1.0f, k);
+            }
+        }
+    }
     for (int f = 0; f < NF; ++f)
         CUDA_TRY(c, cudaMemcpyAsync(s + f * c->N, src[f], sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
     const int bs = 256;
     shift_rho_kernel<<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(s + F_D * c->N, c->n);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
+    if (!fp32) {
+        int rc = io_to_state(c);
+        if (rc) return rc;
+    }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->loaded = true;
     return TSLB_OK;
@@ -397,10 +527,16 @@ int tslb_upload_pops(tslb_ctx* c, const float* f, const float* g) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(dg, g, sizeof(float) * nqg * vol, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
         const int bs = 128;
+        const bool fp32 = c->p.precision == TSLB_PREC_FP32;
+        float* dst = fp32 ? static_cast<float*>(c->state[c->cur]) : c->io;
         pops_to_moments_kernel<<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(
-            c->nx, c->ny, c->nz, c->N, c->p.mode == TSLB_MODE_COLOUR, df, dg, c->state[c->cur]);
+            c->nx, c->ny, c->nz, c->N, c->p.mode == TSLB_MODE_COLOUR, df, dg, dst);
         c->launches++;
         e = cudaGetLastError();
+        if (e == cudaSuccess && !fp32) {
+            default_scales(c);
+            if (io_to_state(c) != TSLB_OK) e = cudaGetLastError();
+        }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(df);
@@ -426,7 +562,9 @@ int tslb_download_moments(tslb_ctx* c, float* rho, float* u, float* v, float* w,
     if (!c) return TSLB_ERR_ARG;
     if (!c->loaded) return fail(c, TSLB_ERR_STATE, "download before an upload");
     float* dst[NF] = {rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi};
-    const float* s = c->state[c->cur];
+    const float* s = nullptr;
+    int rc = fp32_view(c, &s);
+    if (rc) return rc;
     for (int f = 0; f < NF; ++f)
         if (dst[f]) CUDA_TRY(c, cudaMemcpyAsync(dst[f], s + f * c->N, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -453,8 +591,10 @@ int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
     CUDA_TRY(c, cudaMemsetAsync(c->red, 0, sizeof(double) * (RED_SLOTS + 1), c->stream));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    reduce_kernel<<<(unsigned)(sms * 4), 256, 0, c->stream>>>(c->state[c->cur], c->n, c->N,
-                                                               c->p.mode == TSLB_MODE_COLOUR, c->red);
+    const float* view = nullptr;
+    int rc = fp32_view(c, &view);
+    if (rc) return rc;
+    reduce_kernel<<<(unsigned)(sms * 4), 256, 0, c->stream>>>(view, c->n, c->N, c->p.mode == TSLB_MODE_COLOUR, c->red);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     double h[RED_SLOTS + 1];
@@ -538,12 +678,7 @@ int noalloc_setup(int dev, NoallocScratch** out) {
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(normals): ") + cudaGetErrorString(e));
         e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(flags): ") + cudaGetErrorString(e));
-        const int sc = (int)step_smem_bytes(TSLB_MODE_COLOUR), sp = (int)step_smem_bytes(TSLB_MODE_PHASEFIELD);
-        const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        if ((e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true>, attr, sc)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false>, attr, sc)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true>, attr, sp)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false>, attr, sp)) != cudaSuccess)
+        if ((e = set_step_attributes()) != cudaSuccess)
             return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
         s.ready = true;
     }
@@ -568,6 +703,7 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be 16-byte aligned");
     for (int f = 0; f < 6; ++f)
         if (p->bc[f] == TSLB_BC_INLET) return noalloc_fail(TSLB_ERR_UNSUPPORTED, "tslb_step_noalloc: inlet faces are not supported");
+    if (p->precision != TSLB_PREC_FP32) return noalloc_fail(TSLB_ERR_UNSUPPORTED, "tslb_step_noalloc: FP32 storage only");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
@@ -587,6 +723,7 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     view.nrm = sc->normals;
     view.flags = sc->flags;
     view.stream = st;
+    for (int f = 0; f < NF; ++f) view.scale[f] = 1.0f;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
@@ -595,21 +732,11 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     if (p->mode == TSLB_MODE_PHASEFIELD) {
         StepArgs an = make_args(&view, d_in, nullptr);
         const int bs = 256;
-        normals_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(an, sc->normals);
+        normals_kernel<float><<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(an, sc->normals);
         if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("normals launch: ") + cudaGetErrorString(e));
     }
     StepArgs a = make_args(&view, d_in, d_out);
-    dim3 block(TX, TY, 1);
-    dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY, (nz + view.zchunk - 1) / view.zchunk);
-    const bool vec = nx % 4 == 0;
-    const size_t sm = step_smem_bytes(p->mode);
-    if (p->mode == TSLB_MODE_COLOUR) {
-        if (vec) step_kernel<TSLB_MODE_COLOUR, true><<<grid, block, sm, st>>>(a);
-        else step_kernel<TSLB_MODE_COLOUR, false><<<grid, block, sm, st>>>(a);
-    } else {
-        if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true><<<grid, block, sm, st>>>(a);
-        else step_kernel<TSLB_MODE_PHASEFIELD, false><<<grid, block, sm, st>>>(a);
-    }
+    launch_step_kernel(a, p->mode, TSLB_PREC_FP32, st);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
     return TSLB_OK;
 }

@@ -19,7 +19,11 @@
 // so that every pulled population costs a handful of FMAs.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cstdint>
+#include <type_traits>
 
 #include "../../include/tslb.h"
 
@@ -61,9 +65,11 @@ struct FaceBC {
 
 struct StepArgs {
     int nx, ny, nz;
-    long long N;            // field stride (floats)
-    const float* in;        // 11 fields
-    float* out;             // 11 fields
+    long long N;            // field stride (elements)
+    const void* in;         // 11 fields of the storage type
+    void* out;              // 11 fields of the storage type
+    float scale[NF];        // stored = value * scale (fp16 storage; 1 otherwise)
+    float iscale[NF];       // value = stored * iscale
     const float* nrm;       // phase field: interface normals (3 fields of stride N)
     int zchunk;             // target planes per block
     int mode;
@@ -74,6 +80,26 @@ struct StepArgs {
     int wall_phi_mode;
     FaceBC face[6];
     unsigned int* flags;    // bit 0: non-finite moment produced
+};
+
+// Storage types of the moment state: FP32, BF16 or FP16 (scaled).  All
+// arithmetic is FP32; conversion happens on load and store.
+template <class T>
+struct Stor;
+template <>
+struct Stor<float> {
+    static __device__ __forceinline__ float ld(float v) { return v; }
+    static __device__ __forceinline__ float st(float v) { return v; }
+};
+template <>
+struct Stor<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(__nv_bfloat16 v) { return __bfloat162float(v); }
+    static __device__ __forceinline__ __nv_bfloat16 st(float v) { return __float2bfloat16_rn(v); }
+};
+template <>
+struct Stor<__half> {
+    static __device__ __forceinline__ float ld(__half v) { return __half2float(v); }
+    static __device__ __forceinline__ __half st(float v) { return __float2half_rn(v); }
 };
 
 __device__ __forceinline__ long long nidx(const StepArgs& a, int x, int y, int z) {
@@ -101,6 +127,23 @@ __device__ __forceinline__ long long plane_area(const StepArgs& a, int face) {
 // the inlet plane's phi (inlet faces), bc phi (wall_phi_mode 0) or the
 // nearest fluid value (mirror).  The first out-of-range non-periodic axis in
 // x, y, z order names the face.
+// stored value -> FP32 value of field f (fp16 storage carries a per-field scale)
+template <class T>
+__device__ __forceinline__ float cvt_in(T v, const StepArgs& a, int f) {
+    if constexpr (std::is_same<T, __half>::value) return Stor<T>::ld(v) * a.iscale[f];
+    else return Stor<T>::ld(v);
+}
+template <class T>
+__device__ __forceinline__ T cvt_out(float v, const StepArgs& a, int f) {
+    if constexpr (std::is_same<T, __half>::value) return Stor<T>::st(v * a.scale[f]);
+    else return Stor<T>::st(v);
+}
+template <class T>
+__device__ __forceinline__ float ld_field(const StepArgs& a, int f, long long idx) {
+    return cvt_in<T>(__ldg(reinterpret_cast<const T*>(a.in) + f * a.N + idx), a, f);
+}
+
+template <class T>
 __device__ float phi_at(const StepArgs& a, int x, int y, int z) {
     int c[3] = {x, y, z};
     int face = -1;
@@ -116,11 +159,11 @@ __device__ float phi_at(const StepArgs& a, int x, int y, int z) {
             }
         }
     }
-    if (face < 0) return __ldg(a.in + F_PHI * a.N + nidx(a, c[0], c[1], c[2]));
+    if (face < 0) return ld_field<T>(a, F_PHI, nidx(a, c[0], c[1], c[2]));
     const FaceBC& fb = a.face[face];
     if (fb.kind == TSLB_BC_INLET) return __ldg(fb.plane + 3 * plane_area(a, face) + plane_index(a, face, c[0], c[1], c[2]));
     if (a.wall_phi_mode == 0) return fb.phi;
-    return __ldg(a.in + F_PHI * a.N + nidx(a, c[0], c[1], c[2]));
+    return ld_field<T>(a, F_PHI, nidx(a, c[0], c[1], c[2]));
 }
 
 // normal component `comp` at any node: periodic wrap, zero on solid faces
@@ -143,10 +186,10 @@ __device__ __forceinline__ bool interior1(const StepArgs& a, int x, int y, int z
 
 // isotropic gradient 3 sum_i p_i c_i s(x+c_i) of phi
 // (recursive_2c_TSLB3D.f90:555-565; recursive_colorTSLB3D.f90:726-744)
+template <class T>
 __device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
     float gx = 0.f, gy = 0.f, gz = 0.f;
     const bool fast = interior1(a, x, y, z);
-    const float* ph = a.in + F_PHI * a.N;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
@@ -155,7 +198,7 @@ __device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
             for (int dx = -1; dx <= 1; ++dx) {
                 if (dx == 0 && dy == 0 && dz == 0) continue;
                 const float wv = wclass(dx * dx + dy * dy + dz * dz);
-                float s = fast ? __ldg(ph + nidx(a, x + dx, y + dy, z + dz)) : phi_at(a, x + dx, y + dy, z + dz);
+                float s = fast ? ld_field<T>(a, F_PHI, nidx(a, x + dx, y + dy, z + dz)) : phi_at<T>(a, x + dx, y + dy, z + dz);
                 s *= wv;
                 if (dx) gx += dx > 0 ? s : -s;
                 if (dy) gy += dy > 0 ? s : -s;

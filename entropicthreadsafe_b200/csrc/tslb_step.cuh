@@ -149,7 +149,7 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 
 // Regularized or bounce-back populations entering target (x,y,z) from
 // behind non-periodic faces; Kp points at the target's own coefficients.
-template <int MODE>
+template <int MODE, class T>
 __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y, int z,
                                 float* acc) {
     float Kp[NCOEF];
@@ -206,7 +206,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             if (!have_m) {
                 const long long id = nidx(a, x, y, z);
 #pragma unroll
-                for (int f = 0; f < NF; ++f) m[f] = __ldg(a.in + f * a.N + id);
+                for (int f = 0; f < NF; ++f) m[f] = ld_field<T>(a, f, id);
                 have_m = true;
             }
             const FaceBC& fb = a.face[vface];
@@ -274,31 +274,39 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
 }
 
 // ---- shared-memory staging geometry ----
-// Moments and phi are staged with the tile's x range widened to 16-byte
-// chunks: columns x0-4 .. x0+TX+3 (SW = TX + 8 floats per row).
-constexpr int SW = TX + 8;
-constexpr int NCH = SW / 4;                   // 16-byte chunks per row
-constexpr int MROWS = CH;                     // moment rows: y0-1 .. y0+TY
-constexpr int PROWS = TY + 4;                 // phi rows: y0-2 .. y0+TY+1
-constexpr int MAREA = MROWS * SW, PAREA = PROWS * SW;
+// Moments and phi are staged with the tile's x range widened to whole
+// 16-byte chunks of EPC elements: columns x0-EPC .. x0+TX+EPC-1.
 constexpr int NTHR = TX * TY;
 constexpr int NHALO = CAREA - NTHR;           // coefficient nodes on the tile rim (84)
 constexpr int NMOM = NF - 1;                  // moments staged per node (phi comes from the phi ring)
-constexpr int MCOPIES = NMOM * MROWS * NCH;   // 16-byte copies of one moment plane
-constexpr int MROUNDS = (MCOPIES + NTHR - 1) / NTHR;
-constexpr int PCOPIES = PROWS * NCH;          // 16-byte copies of one phi plane
-constexpr int PELEMS = PROWS * SW;
-constexpr int PEROUNDS = (PELEMS + NTHR - 1) / NTHR;
+template <int ES>   // element size in bytes
+struct Geo {
+    static constexpr int EPC = 16 / ES;               // elements per 16-byte chunk
+    static constexpr int SW = TX + 2 * EPC;           // staged row width
+    static constexpr int OFF = EPC - 1;               // staged column of tile column 0 (x0 - 1)
+    static constexpr int NCH = SW / EPC;              // chunks per row
+    static constexpr int MROWS = CH;                  // moment rows: y0-1 .. y0+TY
+    static constexpr int PROWS = TY + 4;              // phi rows: y0-2 .. y0+TY+1
+    static constexpr int MAREA = MROWS * SW, PAREA = PROWS * SW;
+    static constexpr int MCOPIES = NMOM * MROWS * NCH;
+    static constexpr int MROUNDS = (MCOPIES + NTHR - 1) / NTHR;
+    static constexpr int PCOPIES = PROWS * NCH;
+    static constexpr int PELEMS = PROWS * SW;
+    static constexpr int PEROUNDS = (PELEMS + NTHR - 1) / NTHR;
+};
 
-__host__ __device__ constexpr size_t step_smem_bytes(int mode) {
-    return sizeof(float) * 2 * NCOEF * CAREA + sizeof(float) * 2 * NMOM * MAREA +
-           (mode == TSLB_MODE_COLOUR ? sizeof(float) * 4 * PAREA : 0);
+__host__ __device__ constexpr size_t step_smem_bytes_es(int mode, int es) {
+    return sizeof(float) * 2 * NCOEF * CAREA + (size_t)es * 2 * NMOM * CH * (TX + 2 * (16 / es)) +
+           (mode == TSLB_MODE_COLOUR ? (size_t)es * 4 * (TY + 4) * (TX + 2 * (16 / es)) : 0);
 }
+__host__ __device__ constexpr size_t step_smem_bytes(int mode) { return step_smem_bytes_es(mode, 4); }
 
 // gradient 3 sum_i p_i c_i phi(x+c_i) from three phi planes held in shared
-// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch SW)
-__device__ __forceinline__ void grad_smem(const float* pm, const float* p0, const float* pp, float g[3]) {
-    auto P = [&](const float* pl, int dx, int dy) { return pl[dy * SW + dx]; };
+// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch SWv).
+// fp16 storage: the caller multiplies the result by the phi scale.
+template <int SWv, class T>
+__device__ __forceinline__ void grad_smem(const T* pm, const T* p0, const T* pp, float g[3]) {
+    auto P = [&](const T* pl, int dx, int dy) { return Stor<T>::ld(pl[dy * SWv + dx]); };
     const float x1 = P(p0, 1, 0) - P(p0, -1, 0);
     const float x2 = (P(p0, 1, 1) + P(p0, 1, -1) + P(pp, 1, 0) + P(pm, 1, 0)) -
                      (P(p0, -1, 1) + P(p0, -1, -1) + P(pp, -1, 0) + P(pm, -1, 0));
@@ -350,13 +358,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// VEC: nx % 4 == 0, so 16-byte chunks of a row never straddle the x faces
-template <int MODE, bool VEC>
+// T: storage type of the moment state (float, __nv_bfloat16, __half).
+// VEC: nx is a multiple of the 16-byte chunk, so chunks never straddle the
+// x faces and planes are staged with 16-byte cp.async copies.
+template <int MODE, bool VEC, class T>
 __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
+    using G = Geo<sizeof(T)>;
+    constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
     extern __shared__ float4 smem4[];
-    float* coef_base = reinterpret_cast<float*>(smem4);   // [2][NCOEF][CAREA]
-    float* mst = coef_base + 2 * NCOEF * CAREA;           // [2][NMOM][MROWS][SW]
-    float* phis = mst + 2 * NMOM * MAREA;                             // colour: [4][PROWS][SW]
+    float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NCOEF][CAREA]
+    T* mst = reinterpret_cast<T*>(coef_base + 2 * NCOEF * CAREA);     // [2][NMOM][MROWS][SW]
+    T* phis = mst + 2 * NMOM * MAREA;                                 // colour: [4][PROWS][SW]
+    const T* gin = reinterpret_cast<const T*>(a.in);
+    T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * a.zchunk;
@@ -392,8 +406,8 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         ci1 = cy * CW + cx;
     }
     // position of a coefficient node (cx, cy) in the staged planes: moments
-    // row cy, column cx + 3; phi row cy + 1, column cx + 3
-    const int mi0 = (ci0 / CW) * SW + (ci0 % CW) + 3, mi1 = (ci1 / CW) * SW + (ci1 % CW) + 3;
+    // row cy, column cx + OFF; phi row cy + 1, same column
+    const int mi0 = (ci0 / CW) * SW + (ci0 % CW) + G::OFF, mi1 = (ci1 / CW) * SW + (ci1 % CW) + G::OFF;
     const int pi0 = mi0 + SW, pi1 = mi1 + SW;
     const int nnodes = has_rim ? 2 : 1;
 
@@ -409,37 +423,42 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
     // fully behind a non-periodic face, whose ghost values are computed.
     int pch_off = 0;
     bool pch_out = true;
-    if (VEC && tid < PCOPIES) {
-        const int row = tid / NCH, ch = tid % NCH;
-        const XYNode nd = xy_node(a, x0 - 4 + 4 * ch, y0 - 2 + row, xper, yper);
+    if (VEC && tid < G::PCOPIES) {
+        const int row = tid / G::NCH, ch = tid % G::NCH;
+        const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 2 + row, xper, yper);
         pch_off = nd.off;
         pch_out = nd.out;
     }
+    auto ghost = [&](float v) { return cvt_out<T>(v, a, F_PHI); };
     auto stage_phi = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
-        float* slot = phis + (z & 3) * PAREA;
-        const float* ph = a.in + F_PHI * a.N + (long long)gz * plane;
+        T* slot = phis + (z & 3) * PAREA;
+        const T* ph = gin + F_PHI * a.N + (long long)gz * plane;
         if (VEC) {
-            if (tid < PCOPIES) {
-                const int row = tid / NCH, ch = tid % NCH;
-                float* dst = slot + row * SW + 4 * ch;
+            if (tid < G::PCOPIES) {
+                const int row = tid / G::NCH, ch = tid % G::NCH;
+                T* dst = slot + row * SW + EPC * ch;
                 if (!pch_out && !zout) {
-                    cp_async16(dst, ph + pch_off);
+                    cp_async16(reinterpret_cast<float*>(dst), reinterpret_cast<const float*>(ph + pch_off));
                 } else {
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) dst[e] = phi_at(a, x0 - 4 + 4 * ch + e, y0 - 2 + row, z);
+                    for (int e = 0; e < EPC; ++e) dst[e] = ghost(phi_at<T>(a, x0 - EPC + EPC * ch + e, y0 - 2 + row, z));
                 }
             }
         } else {
 #pragma unroll
-            for (int r = 0; r < PEROUNDS; ++r) {
+            for (int r = 0; r < G::PEROUNDS; ++r) {
                 const int j = tid + r * NTHR;
-                if (j < PELEMS) {
+                if (j < G::PELEMS) {
                     const int row = j / SW, col = j % SW;
-                    const XYNode nd = xy_node(a, x0 - 4 + col, y0 - 2 + row, xper, yper);
-                    if (!nd.out && !zout) cp_async4(slot + j, ph + nd.off);
-                    else slot[j] = phi_at(a, nd.gx, nd.gy, z);
+                    const XYNode nd = xy_node(a, x0 - EPC + col, y0 - 2 + row, xper, yper);
+                    if (!nd.out && !zout) {
+                        if constexpr (sizeof(T) == 4) cp_async4(reinterpret_cast<float*>(slot + j), reinterpret_cast<const float*>(ph + nd.off));
+                        else slot[j] = ph[nd.off];
+                    } else {
+                        slot[j] = ghost(phi_at<T>(a, nd.gx, nd.gy, z));
+                    }
                 }
             }
         }
@@ -447,41 +466,45 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
 
     // ---- staging of the 10 non-phi moments of plane z ----
     // VEC: copy j = tid + r NTHR < MCOPIES is (field j / (MROWS NCH), row, chunk)
-    int mch_off[MROUNDS];
+    int mch_off[G::MROUNDS];
     unsigned mch_ok = 0;
     if (VEC) {
 #pragma unroll
-        for (int r = 0; r < MROUNDS; ++r) {
+        for (int r = 0; r < G::MROUNDS; ++r) {
             const int j = tid + r * NTHR;
-            const int rem = j % (MROWS * NCH), row = rem / NCH, ch = rem % NCH;
-            const XYNode nd = xy_node(a, x0 - 4 + 4 * ch, y0 - 1 + row, xper, yper);
+            const int rem = j % (G::MROWS * G::NCH), row = rem / G::NCH, ch = rem % G::NCH;
+            const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 1 + row, xper, yper);
             mch_off[r] = nd.off;
-            if (j < MCOPIES && !nd.out) mch_ok |= 1u << r;
+            if (j < G::MCOPIES && !nd.out) mch_ok |= 1u << r;
         }
     }
     auto stage_mom = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
         if (zout) return;
-        float* dst = mst + (z & 1) * (NMOM * MAREA);
-        const float* src = a.in + (long long)gz * plane;
+        T* dst = mst + (z & 1) * (NMOM * MAREA);
+        const T* src = gin + (long long)gz * plane;
         if (VEC) {
 #pragma unroll
-            for (int r = 0; r < MROUNDS; ++r) {
+            for (int r = 0; r < G::MROUNDS; ++r) {
                 if (!(mch_ok & (1u << r))) continue;
                 const int j = tid + r * NTHR;
-                const int f = j / (MROWS * NCH), rem = j % (MROWS * NCH);
-                const int row = rem / NCH, ch = rem % NCH;
-                cp_async16(dst + f * MAREA + row * SW + 4 * ch, src + f * a.N + mch_off[r]);
+                const int f = j / (G::MROWS * G::NCH), rem = j % (G::MROWS * G::NCH);
+                const int row = rem / G::NCH, ch = rem % G::NCH;
+                cp_async16(reinterpret_cast<float*>(dst + f * MAREA + row * SW + EPC * ch),
+                           reinterpret_cast<const float*>(src + f * a.N + mch_off[r]));
             }
         } else {
             for (int r = 0; r < nnodes; ++r) {
                 const XYNode nd = r ? cn1 : cn0;
                 if (nd.out) continue;
-                const float* p = src + nd.off;
-                float* d = dst + (r ? mi1 : mi0);
+                const T* p = src + nd.off;
+                T* d = dst + (r ? mi1 : mi0);
 #pragma unroll
-                for (int f = 0; f < NMOM; ++f) cp_async4(d + f * MAREA, p + f * a.N);
+                for (int f = 0; f < NMOM; ++f) {
+                    if constexpr (sizeof(T) == 4) cp_async4(reinterpret_cast<float*>(d + f * MAREA), reinterpret_cast<const float*>(p + f * a.N));
+                    else d[f * MAREA] = p[f * a.N];
+                }
             }
         }
     };
@@ -510,12 +533,12 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         if (more) stage_mom(s + 1);
         cp_async_commit();
         cp_async_wait<2>();  // this thread's moment copies of plane s have landed
-        // VEC staging lets any thread copy any node's moments: make them visible
+        // VEC staging lets threads copy other threads' nodes: make the copies visible
         if (VEC) __syncthreads();
         // ---- 1. coefficients of source plane s: own column and one rim node ----
         bool zsolid;
         const int gz = zwrap(s, zsolid);
-        const float* ms = mst + (s & 1) * (NMOM * MAREA);
+        const T* ms = mst + (s & 1) * (NMOM * MAREA);
         // a solid source plane sends nothing: no coefficients, no pull
         for (int r = 0; r < (zsolid ? 0 : nnodes); ++r) {
             const XYNode nd = r ? cn1 : cn0;
@@ -528,18 +551,21 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
             } else {
                 float m[NF];
 #pragma unroll
-                for (int f = 0; f < NMOM; ++f) m[f] = ms[f * MAREA + mi];
+                for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
                 float g[3] = {0.f, 0.f, 0.f};
                 int gx = 0, gy = 0;
                 if (MODE == TSLB_MODE_COLOUR) {
                     const int pi = r ? pi1 : pi0;
-                    const float* p0 = phis + (s & 3) * PAREA + pi;
-                    const float* pm = phis + ((s - 1) & 3) * PAREA + pi;
-                    const float* pp = phis + ((s + 1) & 3) * PAREA + pi;
-                    m[F_PHI] = *p0;
-                    grad_smem(pm, p0, pp, g);
+                    const T* p0 = phis + (s & 3) * PAREA + pi;
+                    const T* pm = phis + ((s - 1) & 3) * PAREA + pi;
+                    const T* pp = phis + ((s + 1) & 3) * PAREA + pi;
+                    m[F_PHI] = cvt_in<T>(*p0, a, F_PHI);
+                    grad_smem<SW>(pm, p0, pp, g);
+                    if constexpr (std::is_same<T, __half>::value) {
+                        g[0] *= a.iscale[F_PHI]; g[1] *= a.iscale[F_PHI]; g[2] *= a.iscale[F_PHI];
+                    }
                 } else {
-                    m[F_PHI] = __ldg(a.in + F_PHI * a.N + (long long)gz * plane + nd.off);
+                    m[F_PHI] = ld_field<T>(a, F_PHI, (long long)gz * plane + nd.off);
                     gx = nd.off % a.nx;
                     gy = nd.off / a.nx;
                 }
@@ -555,10 +581,10 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
                 // own-column phi of the target planes (the ring holds planes s-1 .. s+2)
-                const int po = (ty + 2) * SW + (tx + 4);
-                phm = phis[((s - 1) & 3) * PAREA + po];
-                ph0 = phis[(s & 3) * PAREA + po];
-                php = phis[((s + 1) & 3) * PAREA + po];
+                const int po = (ty + 2) * SW + (tx + EPC);
+                phm = cvt_in<T>(phis[((s - 1) & 3) * PAREA + po], a, F_PHI);
+                ph0 = cvt_in<T>(phis[(s & 3) * PAREA + po], a, F_PHI);
+                php = cvt_in<T>(phis[((s + 1) & 3) * PAREA + po], a, F_PHI);
             }
             if (!zsolid) {
                 pull_row<MODE, -1>(Kc, accm, acc0, accp, phm, ph0, php);
@@ -570,7 +596,7 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
                 unsigned mask = colmask;
                 if (!zper && s == 0) mask |= 16u;
                 if (!zper && s == a.nz - 1) mask |= 32u;
-                if (mask) boundary_target<MODE>(a, Kc, mask, X, Y, s, acc0);
+                if (mask) boundary_target<MODE, T>(a, Kc, mask, X, Y, s, acc0);
             }
             // ---- 4. target plane s-1 is complete ----
             const int t = s - 1;
@@ -589,12 +615,13 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
                 o[F_YZ] = accm[A_YZ] - rho * v * w;
                 // colour mode: phi_t + (colour increment) / rho
                 o[F_PHI] = MODE == TSLB_MODE_COLOUR ? fmaf(accm[A_COL], inv, phm) : accm[A_COL];
-                float* po = a.out + (long long)t * plane + cn0.off;
+                T* po = gout + (long long)t * plane + cn0.off;
                 float chk = 0.f;
 #pragma unroll
                 for (int f = 0; f < NF; ++f) {
-                    po[f * a.N] = o[f];
-                    chk += o[f];
+                    const T st = cvt_out<T>(o[f], a, f);
+                    po[f * a.N] = st;
+                    chk += Stor<T>::ld(st);
                 }
                 if (!isfinite(chk)) atomicOr(a.flags, 1u);
             }

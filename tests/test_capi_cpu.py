@@ -44,7 +44,7 @@ def test_default_params_match_python_mirror(lib):
     ("tau_a", 0.5, capi.ERR_ARG),
     ("tau_a", float("nan"), capi.ERR_ARG),
     ("mode", 7, capi.ERR_ARG),
-    ("precision", capi.PREC_BF16, capi.ERR_UNSUPPORTED),
+    ("precision", 7, capi.ERR_ARG),
     ("wall_phi_mode", 3, capi.ERR_ARG),
 ])
 def test_create_rejects_bad_params(lib, field, value, code):
