@@ -214,6 +214,58 @@ def e2e_run(args, p, f, ws):
                     "+ tslb_download_moments, wall clock, per step"}
 
 
+def ensemble_leg(args, ndomains: int = 48):
+    """Config 4: 48 droplet-in-Couette domains of uneven size advanced by one
+    launch per step (K steps from a CUDA graph, tuned z chunk and grid),
+    against the same domains launched one at a time."""
+    import torch
+    from entropicthreadsafe_b200 import ensemble
+    from entropicthreadsafe_b200.solver import Lattice
+    doms = ensemble.couette_droplets(n=ndomains, seed=2024)
+    nodes = sum(a * b * c for a, b, c in (d["dims"] for d in doms))
+    with ensemble.Ensemble([d["params"] for d in doms], [d["dims"] for d in doms]) as ens:
+        for i, d in enumerate(doms):
+            ens.upload_moments(i, d["fields"])
+        zc, gr = ens.tune()
+        st = torch.cuda.ExternalStream(ens.stream)
+        k = args.steps if args.steps % 2 == 0 else args.steps + 1
+        ens.step_graph(k)  # capture + warm-up
+        ens.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ens.step_graph(k)
+        e1.record(st)
+        ens.synchronize()
+        ms_graph = e0.elapsed_time(e1) / k
+        e0.record(st)
+        ens.step(k)
+        e1.record(st)
+        ens.synchronize()
+        ms_plain = e0.elapsed_time(e1) / k
+    # the same domains, one lattice at a time
+    lats = []
+    for d in doms:
+        nx, ny, nz = d["dims"]
+        lat = Lattice(d["params"], nx, ny, nz)
+        lat.upload_moments(d["fields"])
+        lat.step(1)
+        lat.synchronize()
+        lats.append(lat)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for lat in lats:
+        lat.step(k)
+        lat.synchronize()
+    ms_seq = (time.perf_counter() - t0) * 1e3 / k
+    for lat in lats:
+        lat.close()
+    return {"domains": ndomains, "nodes": nodes, "steps": k, "tuned": {"zchunk": zc, "grid": gr},
+            "value_graph": nodes / (ms_graph * 1e-3) / 1e6, "value_launch_per_step": nodes / (ms_plain * 1e-3) / 1e6,
+            "value_one_at_a_time": nodes / (ms_seq * 1e-3) / 1e6, "unit": UNIT,
+            "speedup_vs_one_at_a_time": ms_seq / ms_graph}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -294,6 +346,7 @@ def run_ours(args):
     # ---- end to end through the public API with host buffers ----
     if lat is not None:
         lat.close()
+    ens = None if args.no_ensemble else ensemble_leg(args)
     barrier_sync()
     e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     state_bytes = 11 * 4 * nodes
@@ -319,7 +372,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}", "l2": "state 830 MB > 126 MB L2, no flush needed",
                    "state_bytes": state_bytes},
         "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-        "precision_forms": forms,
+        "precision_forms": forms, "ensemble": ens,
         "clocks": clk, "check": {"mass": red["mass"], "umax": red["umax"], "mass_a": red["mass_a"]},
     }
     print(json.dumps(line), flush=True)
@@ -338,6 +391,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-precision-forms", action="store_true", help="skip the bf16 / fp16 storage legs")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-domain ensemble leg")
     ap.add_argument("--nz", type=int, default=0, help="shallower channel (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -130,6 +130,28 @@ def lib() -> ctypes.CDLL:
         L.tslb_last_error.restype = ctypes.c_char_p
         L.tslb_step_noalloc.argtypes = [vp, ip, ip, ip, vp, vp, ctypes.c_longlong, vp]
         L.tslb_step_noalloc.restype = ip
+        L.tslb_ensemble_create.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ip, ctypes.POINTER(vp)]
+        L.tslb_ensemble_create.restype = ip
+        L.tslb_ensemble_destroy.argtypes = [vp]
+        L.tslb_ensemble_destroy.restype = None
+        L.tslb_ensemble_upload_moments.argtypes = [vp, ip] + [fp] * 11
+        L.tslb_ensemble_upload_moments.restype = ip
+        L.tslb_ensemble_download_moments.argtypes = [vp, ip] + [fp] * 11
+        L.tslb_ensemble_download_moments.restype = ip
+        L.tslb_ensemble_step.argtypes = [vp, ip]
+        L.tslb_ensemble_step.restype = ip
+        L.tslb_ensemble_step_graph.argtypes = [vp, ip]
+        L.tslb_ensemble_step_graph.restype = ip
+        L.tslb_ensemble_reduce.argtypes = [vp, ip, dp]
+        L.tslb_ensemble_reduce.restype = ip
+        L.tslb_ensemble_tune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.tslb_ensemble_tune.restype = ip
+        L.tslb_ensemble_synchronize.argtypes = [vp]
+        L.tslb_ensemble_synchronize.restype = ip
+        L.tslb_ensemble_stream.argtypes = [vp]
+        L.tslb_ensemble_stream.restype = vp
+        L.tslb_ensemble_last_error.argtypes = [vp]
+        L.tslb_ensemble_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
 

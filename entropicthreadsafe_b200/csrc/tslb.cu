@@ -740,3 +740,366 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
     return TSLB_OK;
 }
+
+// ------------------------------------------------------ batched ensemble
+struct tslb_ensemble {
+    std::vector<tslb_ctx*> m;          // member lattices (own state, own params)
+    int mode = 0, precision = 0;
+    bool vec = true;
+    cudaStream_t stream = nullptr;
+    StepArgs* d_args[2] = {nullptr, nullptr};  // per step parity: member args
+    WorkItem* d_work = nullptr;
+    int nwork = 0;
+    int zchunk = 16;
+    int grid = 0;                      // 0: one block per work item
+    int sms = 148;
+    int parity = 0;                    // steps taken mod 2 since the last args upload
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    std::string err;
+};
+
+namespace {
+
+int efail(tslb_ensemble* e, int code, const std::string& msg) {
+    if (e) e->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define ECUDA_TRY(e, call)                                                               \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return efail(e, TSLB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void ens_drop_graph(tslb_ensemble* e) {
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+    e->graph_steps = 0;
+}
+
+// Rebuild the work list and both parities of the member arguments for the
+// current z chunk and member buffers.
+int ens_build(tslb_ensemble* e) {
+    std::vector<WorkItem> work;
+    std::vector<StepArgs> args[2];
+    for (size_t d = 0; d < e->m.size(); ++d) {
+        tslb_ctx* c = e->m[d];
+        c->zchunk = std::min(e->zchunk, c->nz);
+        const int gx = (c->nx + TX - 1) / TX, gy = (c->ny + TY - 1) / TY, gz = (c->nz + c->zchunk - 1) / c->zchunk;
+        for (int bz = 0; bz < gz; ++bz)
+            for (int by = 0; by < gy; ++by)
+                for (int bx = 0; bx < gx; ++bx) work.push_back(WorkItem{(int)d, bx, by, bz});
+        for (int par = 0; par < 2; ++par) {
+            const int cur = c->cur ^ par;
+            args[par].push_back(make_args(c, c->state[cur], c->state[cur ^ 1]));
+        }
+    }
+    ens_drop_graph(e);
+    cudaFree(e->d_work);
+    for (int par = 0; par < 2; ++par) cudaFree(e->d_args[par]);
+    e->d_work = nullptr;
+    e->d_args[0] = e->d_args[1] = nullptr;
+    e->nwork = (int)work.size();
+    ECUDA_TRY(e, cudaMalloc(&e->d_work, sizeof(WorkItem) * work.size()));
+    ECUDA_TRY(e, cudaMemcpy(e->d_work, work.data(), sizeof(WorkItem) * work.size(), cudaMemcpyHostToDevice));
+    for (int par = 0; par < 2; ++par) {
+        ECUDA_TRY(e, cudaMalloc(&e->d_args[par], sizeof(StepArgs) * args[par].size()));
+        ECUDA_TRY(e, cudaMemcpy(e->d_args[par], args[par].data(), sizeof(StepArgs) * args[par].size(), cudaMemcpyHostToDevice));
+    }
+    e->parity = 0;
+    return TSLB_OK;
+}
+
+// one ensemble step on the ensemble stream (no host synchronisation)
+int ens_launch(tslb_ensemble* e) {
+    if (e->mode == TSLB_MODE_PHASEFIELD) {
+        for (tslb_ctx* c : e->m) {
+            StepArgs a = make_args(c, c->state[c->cur ^ e->parity], nullptr);
+            const int bs = 256;
+            with_storage(e->precision, [&](auto tag) {
+                normals_kernel<decltype(tag)><<<(unsigned)((c->n + bs - 1) / bs), bs, 0, e->stream>>>(a, c->nrm);
+            });
+        }
+    }
+    const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
+    const StepArgs* args = e->d_args[e->parity];
+    with_storage(e->precision, [&](auto tag) {
+        using T = decltype(tag);
+        const size_t sm = step_smem_bytes_es(e->mode, (int)sizeof(T));
+        dim3 block(TX, TY, 1);
+        if (e->mode == TSLB_MODE_COLOUR) {
+            if (e->vec) ensemble_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
+            else ensemble_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
+        } else {
+            if (e->vec) ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
+            else ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
+        }
+    });
+    ECUDA_TRY(e, cudaGetLastError());
+    e->parity ^= 1;
+    return TSLB_OK;
+}
+
+// fold the steps taken into the members' current buffers
+void ens_settle(tslb_ensemble* e) {
+    if (e->parity) {
+        for (tslb_ctx* c : e->m) c->cur ^= 1;
+        // arguments of parity 0 must again start from the members' current buffers
+        std::swap(e->d_args[0], e->d_args[1]);
+        e->parity = 0;
+    }
+}
+
+cudaError_t ens_set_attributes() {
+    cudaError_t err = cudaSuccess;
+    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    auto one = [&](auto tag) {
+        using T = decltype(tag);
+        const int es = (int)sizeof(T);
+        const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, es), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, es);
+        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_COLOUR, true, T>, attr, sc);
+        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_COLOUR, false, T>, attr, sc);
+        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T>, attr, sp);
+        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T>, attr, sp);
+    };
+    one(float{});
+    one(__nv_bfloat16{});
+    one(__half{});
+    return err;
+}
+
+int ens_check(tslb_ensemble* e, int i) {
+    if (!e) return TSLB_ERR_ARG;
+    if (i < 0 || i >= (int)e->m.size()) return efail(e, TSLB_ERR_ARG, "member index out of range");
+    return TSLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb_ensemble** out) {
+    if (!out) return efail(nullptr, TSLB_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!params || !dims || n < 1) return efail(nullptr, TSLB_ERR_ARG, "tslb_ensemble_create: need n >= 1 members");
+    for (int i = 1; i < n; ++i)
+        if (params[i].mode != params[0].mode || params[i].precision != params[0].precision)
+            return efail(nullptr, TSLB_ERR_ARG, "tslb_ensemble_create: members must share mode and precision");
+    for (int i = 0; i < n; ++i)
+        for (int f = 0; f < 6; ++f)
+            if (params[i].bc[f] == TSLB_BC_INLET)
+                return efail(nullptr, TSLB_ERR_UNSUPPORTED, "tslb_ensemble_create: inlet faces are not supported in ensembles");
+    tslb_ensemble* e = new (std::nothrow) tslb_ensemble();
+    if (!e) return efail(nullptr, TSLB_ERR_ARG, "out of host memory");
+    e->mode = params[0].mode;
+    e->precision = params[0].precision;
+    for (int i = 0; i < n; ++i) {
+        tslb_ctx* c = nullptr;
+        int rc = tslb_create(&params[i], dims[3 * i], dims[3 * i + 1], dims[3 * i + 2], &c);
+        if (rc) {
+            std::string msg = "member " + std::to_string(i) + ": " + g_create_error;
+            tslb_ensemble_destroy(e);
+            return efail(nullptr, rc, msg);
+        }
+        e->m.push_back(c);
+        const int epc = 16 / storage_bytes(e->precision);
+        if (dims[3 * i] % epc) e->vec = false;
+    }
+    cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = ens_set_attributes();
+    int dev = 0;
+    if (ce == cudaSuccess) ce = cudaGetDevice(&dev);
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (ce != cudaSuccess) {
+        std::string msg = std::string("tslb_ensemble_create: ") + cudaGetErrorString(ce);
+        tslb_ensemble_destroy(e);
+        return efail(nullptr, TSLB_ERR_CUDA, msg);
+    }
+    e->grid = 2 * e->sms;  // persistent: two resident blocks per SM walk the work list
+    int rc = ens_build(e);
+    if (rc) {
+        std::string msg = e->err;
+        tslb_ensemble_destroy(e);
+        return efail(nullptr, rc, msg);
+    }
+    *out = e;
+    return TSLB_OK;
+}
+
+void tslb_ensemble_destroy(tslb_ensemble* e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    ens_drop_graph(e);
+    cudaFree(e->d_work);
+    for (int par = 0; par < 2; ++par) cudaFree(e->d_args[par]);
+    for (tslb_ctx* c : e->m) tslb_destroy(c);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int tslb_ensemble_upload_moments(tslb_ensemble* e, int i, const float* rho, const float* u, const float* v,
+                                 const float* w, const float* pxx, const float* pxy, const float* pxz,
+                                 const float* pyy, const float* pyz, const float* pzz, const float* phi) {
+    int rc = ens_check(e, i);
+    if (rc) return rc;
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    rc = tslb_upload_moments(e->m[i], rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi);
+    if (rc) return efail(e, rc, e->m[i]->err);
+    // fp16 scales may have changed: refresh the member arguments
+    return ens_build(e);
+}
+
+int tslb_ensemble_step(tslb_ensemble* e, int nsteps) {
+    if (!e) return TSLB_ERR_ARG;
+    if (nsteps < 0) return efail(e, TSLB_ERR_ARG, "nsteps < 0");
+    for (tslb_ctx* c : e->m)
+        if (!c->loaded) return efail(e, TSLB_ERR_STATE, "tslb_ensemble_step before every member is uploaded");
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = ens_launch(e);
+        if (rc) return rc;
+    }
+    return TSLB_OK;
+}
+
+int tslb_ensemble_step_graph(tslb_ensemble* e, int nsteps) {
+    if (!e) return TSLB_ERR_ARG;
+    if (nsteps < 1) return efail(e, TSLB_ERR_ARG, "nsteps < 1");
+    for (tslb_ctx* c : e->m)
+        if (!c->loaded) return efail(e, TSLB_ERR_STATE, "tslb_ensemble_step_graph before every member is uploaded");
+    if (!e->graph || e->graph_steps != nsteps || e->parity != 0) {
+        ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+        ens_settle(e);
+        ens_drop_graph(e);
+        cudaGraph_t g = nullptr;
+        ECUDA_TRY(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = TSLB_OK;
+        for (int s = 0; s < nsteps && rc == TSLB_OK; ++s) rc = ens_launch(e);
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        e->parity = 0;  // capture records launches; they have not run
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ce != cudaSuccess) return efail(e, TSLB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return efail(e, TSLB_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce));
+        e->graph_steps = nsteps;
+    }
+    ECUDA_TRY(e, cudaGraphLaunch(e->graph, e->stream));
+    // the graph starts and ends on parity 0 only for even nsteps
+    if (nsteps % 2) {
+        ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+        for (tslb_ctx* c : e->m) c->cur ^= 1;
+        std::swap(e->d_args[0], e->d_args[1]);
+        ens_drop_graph(e);
+    }
+    return TSLB_OK;
+}
+
+int tslb_ensemble_download_moments(tslb_ensemble* e, int i, float* rho, float* u, float* v, float* w, float* pxx,
+                                   float* pxy, float* pxz, float* pyy, float* pyz, float* pzz, float* phi) {
+    int rc = ens_check(e, i);
+    if (rc) return rc;
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    rc = tslb_download_moments(e->m[i], rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi);
+    if (rc) return efail(e, rc, e->m[i]->err);
+    return TSLB_OK;
+}
+
+int tslb_ensemble_reduce(tslb_ensemble* e, int i, double out[TSLB_NREDUCE]) {
+    int rc = ens_check(e, i);
+    if (rc) return rc;
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    rc = tslb_reduce(e->m[i], out);
+    if (rc) return efail(e, rc, e->m[i]->err);
+    return TSLB_OK;
+}
+
+int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
+    if (!e) return TSLB_ERR_ARG;
+    for (tslb_ctx* c : e->m)
+        if (!c->loaded) return efail(e, TSLB_ERR_STATE, "tslb_ensemble_tune before every member is uploaded");
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    // back up every member's current state; tuning steps run on it and it is restored
+    std::vector<void*> backup(e->m.size(), nullptr);
+    auto release = [&]() { for (void* b : backup) cudaFree(b); };
+    for (size_t d = 0; d < e->m.size(); ++d) {
+        tslb_ctx* c = e->m[d];
+        const size_t bytes = (size_t)c->esize * NF * c->N;
+        cudaError_t ce = cudaMalloc(&backup[d], bytes);
+        if (ce == cudaSuccess) ce = cudaMemcpy(backup[d], c->state[c->cur], bytes, cudaMemcpyDeviceToDevice);
+        if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
+    }
+    const int zcands[] = {8, 16, 32, 64, 128, 1 << 20};
+    const int gcands[] = {2 * e->sms, 0};
+    float best = 1e30f;
+    int bz = e->zchunk, bg = e->grid;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    int rc = TSLB_OK;
+    for (int zc : zcands) {
+        for (int gr : gcands) {
+            e->zchunk = zc;
+            e->grid = gr;
+            rc = ens_build(e);
+            if (rc) break;
+            const int reps = 4;
+            rc = ens_launch(e);  // warm-up
+            cudaEventRecord(t0, e->stream);
+            for (int r = 0; r < reps && rc == TSLB_OK; ++r) rc = ens_launch(e);
+            cudaEventRecord(t1, e->stream);
+            cudaError_t ce = cudaEventSynchronize(t1);
+            if (rc == TSLB_OK && ce != cudaSuccess) rc = efail(e, TSLB_ERR_CUDA, std::string("tune: ") + cudaGetErrorString(ce));
+            if (rc) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            if (ms < best) { best = ms; bz = zc; bg = gr; }
+            // keep the members' buffers consistent with their cur index
+            ens_settle(e);
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    // restore the uploaded state
+    for (size_t d = 0; d < e->m.size() && rc == TSLB_OK; ++d) {
+        tslb_ctx* c = e->m[d];
+        cudaError_t ce = cudaMemcpy(c->state[c->cur], backup[d], (size_t)c->esize * NF * c->N, cudaMemcpyDeviceToDevice);
+        if (ce != cudaSuccess) rc = efail(e, TSLB_ERR_CUDA, std::string("tune restore: ") + cudaGetErrorString(ce));
+    }
+    release();
+    if (rc) return rc;
+    e->zchunk = bz;
+    e->grid = bg;
+    rc = ens_build(e);
+    if (rc) return rc;
+    if (zchunk_out) *zchunk_out = bz;
+    if (grid_out) *grid_out = bg;
+    return TSLB_OK;
+}
+
+int tslb_ensemble_synchronize(tslb_ensemble* e) {
+    if (!e) return TSLB_ERR_ARG;
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    for (tslb_ctx* c : e->m) {
+        int rc = check_flags(c);
+        if (rc) return efail(e, rc, c->err);
+    }
+    return TSLB_OK;
+}
+
+void* tslb_ensemble_stream(tslb_ensemble* e) { return e ? (void*)e->stream : nullptr; }
+
+const char* tslb_ensemble_last_error(tslb_ensemble* e) {
+    if (!e) return g_create_error.c_str();
+    return e->err.c_str();
+}
+
+}  // extern "C"

@@ -361,8 +361,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // T: storage type of the moment state (float, __nv_bfloat16, __half).
 // VEC: nx is a multiple of the 16-byte chunk, so chunks never straddle the
 // x faces and planes are staged with 16-byte cp.async copies.
+// One block's work: tile (bx, by) of columns and z chunk bz of lattice a.
 template <int MODE, bool VEC, class T>
-__global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
+__device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, int bz) {
     using G = Geo<sizeof(T)>;
     constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
     extern __shared__ float4 smem4[];
@@ -372,8 +373,8 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
     const T* gin = reinterpret_cast<const T*>(a.in);
     T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int z0 = blockIdx.z * a.zchunk;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int z0 = bz * a.zchunk;
     const int z1 = min(z0 + a.zchunk, a.nz);
     const int X = x0 + tx, Y = y0 + ty;
     const bool active = X < a.nx && Y < a.ny;
@@ -632,6 +633,41 @@ __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
         buf ^= 1;
     }
     cp_async_wait<0>();
+}
+
+template <int MODE, bool VEC, class T>
+__global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
+    step_block<MODE, VEC, T>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Work item of the ensemble kernel: lattice, tile column, z chunk.
+struct WorkItem {
+    int dom, bx, by, bz;
+};
+
+// Ensemble step: blocks walk a list of work items over many independent
+// lattices (stride gridDim.x); each item is one tile column and z chunk of
+// one lattice.  The lattice's arguments are staged in shared memory when the
+// block moves to a new lattice.  All lattices share MODE, VEC and T.
+template <int MODE, bool VEC, class T>
+__global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __restrict__ args,
+                                                          const WorkItem* __restrict__ work, int nwork) {
+    __shared__ StepArgs sa;
+    int cur = -1;
+    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+        const WorkItem w = work[it];
+        if (w.dom != cur) {
+            __syncthreads();
+            const int words = (int)(sizeof(StepArgs) / sizeof(int));
+            const int* src = reinterpret_cast<const int*>(args + w.dom);
+            int* dst = reinterpret_cast<int*>(&sa);
+            for (int i = threadIdx.y * TX + threadIdx.x; i < words; i += NTHR) dst[i] = src[i];
+            __syncthreads();
+            cur = w.dom;
+        }
+        step_block<MODE, VEC, T>(sa, w.bx, w.by, w.bz);
+        __syncthreads();
+    }
 }
 
 }  // namespace tslb

@@ -178,6 +178,40 @@ long long tslb_launch_count(tslb_ctx* ctx);
  * last failed tslb_create or tslb_step_noalloc).  Never NULL. */
 const char* tslb_last_error(tslb_ctx* ctx);
 
+/* ---- batched ensemble of independent lattices ----
+ *
+ * Many independent lattices of different sizes (all of one mode and one
+ * storage precision) advanced together: every time step is ONE kernel
+ * launch whose blocks walk a work list of (lattice, tile, z chunk) items,
+ * and tslb_ensemble_step_graph captures K such steps in a CUDA graph.  This
+ * replaces running the reference program once per domain (the reference
+ * has no batching).  Member i is addressed by its index. */
+typedef struct tslb_ensemble tslb_ensemble;
+
+/* params[i] and dims[3*i .. 3*i+2] = (nx, ny, nz) of member i. */
+int  tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb_ensemble** out);
+void tslb_ensemble_destroy(tslb_ensemble* e);
+int  tslb_ensemble_upload_moments(tslb_ensemble* e, int i,
+                                  const float* rho, const float* u, const float* v, const float* w,
+                                  const float* pxx, const float* pxy, const float* pxz,
+                                  const float* pyy, const float* pyz, const float* pzz,
+                                  const float* phi);
+/* nsteps steps, one launch each, on the ensemble stream (asynchronous). */
+int  tslb_ensemble_step(tslb_ensemble* e, int nsteps);
+/* The same nsteps steps replayed from a CUDA graph (captured on first use). */
+int  tslb_ensemble_step_graph(tslb_ensemble* e, int nsteps);
+int  tslb_ensemble_download_moments(tslb_ensemble* e, int i,
+                                    float* rho, float* u, float* v, float* w,
+                                    float* pxx, float* pxy, float* pxz,
+                                    float* pyy, float* pyz, float* pzz, float* phi);
+int  tslb_ensemble_reduce(tslb_ensemble* e, int i, double out[TSLB_NREDUCE]);
+/* Autotuner: time the candidate z chunks and grid sizes on the uploaded
+ * state (restored afterwards) and keep the fastest; returns the choice. */
+int  tslb_ensemble_tune(tslb_ensemble* e, int* zchunk, int* grid);
+int  tslb_ensemble_synchronize(tslb_ensemble* e);
+void* tslb_ensemble_stream(tslb_ensemble* e);
+const char* tslb_ensemble_last_error(tslb_ensemble* e);
+
 /* Largest lattice (nodes) tslb_step_noalloc accepts. */
 #define TSLB_NOALLOC_MAX_NODES (1LL << 20)
 
