@@ -1,47 +1,67 @@
 """Build libtslb.so in-tree with nvcc for sm_100a (B200).
 
     python -m entropicthreadsafe_b200.build [--verbose]
+
+Each csrc/*.cu is compiled to an object under csrc/_build (in parallel),
+then linked into entropicthreadsafe_b200/libtslb.so with the static CUDA
+runtime.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(CSRC, "_build")
 OUT = os.path.join(HERE, "libtslb.so")
-SOURCES = ["tslb.cu"]
-HEADERS = ["tslb_device.cuh", "tslb_step.cuh"]
+SOURCES = ["tslb.cu", "closure.cu"]
+HEADERS = ["tslb_device.cuh", "tslb_step.cuh", "tslb_internal.h", "tcgen05.cuh", "closure_mlp.cuh"]
+INCLUDES = ["tslb.h", "tslb_closure.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
-    "-Xptxas", "-v",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
+
+
+def _deps() -> list:
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps += [os.path.join(HERE, "..", "include", f) for f in INCLUDES]
+    return [d for d in deps if os.path.exists(d)]
 
 
 def _stale() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(HERE, "..", "include", "tslb.h"))
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(os.path.getmtime(d) > t for d in _deps())
+
+
+def _compile(src: str):
+    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    cmd = [NVCC] + CFLAGS + ["-c", "-o", obj, os.path.join(CSRC, src)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    return obj, cmd, res
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile csrc/*.cu into libtslb.so next to this file; returns its path."""
     if not force and not _stale():
         return OUT
-    cmd = [NVCC] + FLAGS + ["-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    os.makedirs(OBJ, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(_compile, SOURCES))
+    for obj, cmd, res in results:
+        if res.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+        if verbose:
+            print(" ".join(cmd))
+            print(res.stderr)
+    link = [NVCC] + ARCH + ["-shared", "-o", OUT] + [r[0] for r in results]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
-    if verbose:
-        print(" ".join(cmd))
-        print(res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + " ".join(link) + "\n" + res.stdout + res.stderr)
     return OUT
 
 

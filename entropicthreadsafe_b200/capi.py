@@ -87,6 +87,40 @@ def make_params(**kw) -> TslbParams:
     return p
 
 
+# learned closure (include/tslb_closure.h)
+CLOSURE_NFEAT = 10
+CLOSURE_HIDDEN = 64
+CLOSURE_OFF = {"W1": 0, "b1": 1024, "W2": 1088, "b2": 5184, "w3": 5248, "b3": 5312}
+CLOSURE_NPARAM = 5313
+
+
+def _declare_closure(L) -> None:
+    vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)
+    ll, dp = ctypes.c_longlong, ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "tslb_closure_create": ([ctypes.POINTER(vp)], ip),
+        "tslb_closure_destroy": ([vp], None),
+        "tslb_closure_set_params": ([vp, fp, fp, fp, ctypes.c_float], ip),
+        "tslb_closure_get_params": ([vp, fp, fp, fp, fp], ip),
+        "tslb_closure_forward": ([vp, fp, ll, fp], ip),
+        "tslb_closure_gradient": ([vp, fp, fp, fp, ll, fp, dp], ip),
+        "tslb_closure_dataset_clear": ([vp], ip),
+        "tslb_closure_dataset_add": ([vp, fp, fp, fp, ll], ip),
+        "tslb_closure_dataset_add_fine": ([vp, vp, ctypes.c_float, ip, ctypes.POINTER(ll)], ip),
+        "tslb_closure_dataset_size": ([vp], ll),
+        "tslb_closure_dataset_download": ([vp, fp, fp, fp], ip),
+        "tslb_closure_normalize": ([vp], ip),
+        "tslb_closure_train": ([vp, ip, ip, ctypes.c_float, ctypes.c_ulonglong, fp], ip),
+        "tslb_closure_features": ([vp, vp, fp], ip),
+        "tslb_attach_closure": ([vp, vp, ip], ip),
+        "tslb_closure_last_error": ([vp], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+
+
 _lib = None
 
 
@@ -152,6 +186,18 @@ def lib() -> ctypes.CDLL:
         L.tslb_ensemble_stream.restype = vp
         L.tslb_ensemble_last_error.argtypes = [vp]
         L.tslb_ensemble_last_error.restype = ctypes.c_char_p
+        lp = ctypes.POINTER(ctypes.c_longlong)
+        L.tslb_set_tau_correction.argtypes = [vp, fp]
+        L.tslb_set_tau_correction.restype = ip
+        L.tslb_download_tau_correction.argtypes = [vp, fp]
+        L.tslb_download_tau_correction.restype = ip
+        L.tslb_stats_reset.argtypes = [vp]
+        L.tslb_stats_reset.restype = ip
+        L.tslb_stats_accumulate.argtypes = [vp]
+        L.tslb_stats_accumulate.restype = ip
+        L.tslb_stats_download.argtypes = [vp, ip, fp, fp, fp, fp, fp, lp]
+        L.tslb_stats_download.restype = ip
+        _declare_closure(L)
         _lib = L
     return _lib
 

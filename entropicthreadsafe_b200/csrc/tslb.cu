@@ -8,45 +8,31 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <string>
 #include <vector>
 
 #include "../../include/tslb.h"
+#include "tslb_internal.h"
 #include "tslb_step.cuh"
 
 using namespace tslb;
 
-struct tslb_ctx {
-    tslb_params p;
-    int nx, ny, nz;
-    long long n;        // nodes
-    long long N;        // padded field stride
-    int device;
-    cudaStream_t stream = nullptr;
-    void* state[2] = {nullptr, nullptr};   // ping-pong, 11 fields each, storage type
-    int esize = 4;                         // bytes per stored element
-    float* io = nullptr;                   // FP32 conversion buffer (bf16/fp16 storage)
-    float scale[NF];                       // fp16 storage: stored = value * scale
-    int cur = 0;
-    float* nrm = nullptr;                  // 3 fields
-    float* inlet[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    unsigned int* flags = nullptr;
-    double* red = nullptr;                 // reduction accumulators
-    bool loaded = false;
-    int zchunk = 32;
-    long long launches = 0;
-    std::string err;
-};
-
 static std::string g_create_error;
 
-namespace {
+namespace tslb_internal {
 
 int fail(tslb_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     else g_create_error = msg;
     return code;
 }
+
+}  // namespace tslb_internal
+
+namespace {
+
+using tslb_internal::fail;
 
 #define CUDA_TRY(ctx, call)                                                              \
     do {                                                                                 \
@@ -109,6 +95,7 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
         a.face[f].plane = c->inlet[f];
     }
     a.flags = c->flags;
+    a.dtau = c->dtau_on ? c->dtau : nullptr;
     for (int f = 0; f < NF; ++f) {
         a.scale[f] = c->scale[f];
         a.iscale[f] = 1.0f / c->scale[f];
@@ -263,14 +250,45 @@ __global__ void reduce_kernel(const float* __restrict__ s, long long n, long lon
     }
 }
 
+// running sums of u, v, w, phi and w^2 (time averages of the jet statistics)
+__global__ void stats_accumulate_kernel(const float* __restrict__ s, long long n, long long N, float* __restrict__ acc) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float w = s[F_W * N + i];
+    acc[i] += s[F_U * N + i];
+    acc[N + i] += s[F_V * N + i];
+    acc[2 * N + i] += w;
+    acc[3 * N + i] += s[F_PHI * N + i];
+    acc[4 * N + i] += w * w;
+}
+
+// means over cf^3 blocks of the running sums: out[k * nc + j], k = u, v, w, phi, w^2
+__global__ void stats_coarsen_kernel(const float* __restrict__ acc, int nx, int ny, int nz, long long N, int cf,
+                                     float inv, float* __restrict__ out) {
+    const int cx = nx / cf, cy = ny / cf, cz = nz / cf;
+    const long long nc = (long long)cx * cy * cz;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= nc) return;
+    const int X = (int)(j % cx), Y = (int)((j / cx) % cy), Z = (int)(j / ((long long)cx * cy));
+    float sum[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int dz = 0; dz < cf; ++dz)
+        for (int dy = 0; dy < cf; ++dy)
+            for (int dx = 0; dx < cf; ++dx) {
+                const long long i = (long long)(cf * X + dx) + (long long)nx * ((cf * Y + dy) + (long long)ny * (cf * Z + dz));
+#pragma unroll
+                for (int k = 0; k < 5; ++k) sum[k] += acc[k * N + i];
+            }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k * nc + j] = sum[k] * inv;
+}
+
 int check_flags(tslb_ctx* c) {
     unsigned int h = 0;
     CUDA_TRY(c, cudaMemcpyAsync(&h, c->flags, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (h & 1u) {
-        CUDA_TRY(c, cudaMemsetAsync(c->flags, 0, sizeof(unsigned int), c->stream));
-        return fail(c, TSLB_ERR_NAN, "the step produced a non-finite moment");
-    }
+    if (h) CUDA_TRY(c, cudaMemsetAsync(c->flags, 0, sizeof(unsigned int), c->stream));
+    if (h & 2u) return fail(c, TSLB_ERR_TIMEOUT, "a bounded wait of the closure kernel ran out");
+    if (h & 1u) return fail(c, TSLB_ERR_NAN, "the step produced a non-finite moment");
     return TSLB_OK;
 }
 
@@ -300,6 +318,9 @@ cudaError_t set_step_attributes() {
     one(float{});
     one(__nv_bfloat16{});
     one(__half{});
+    const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, 4);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, float, true>, attr, sc);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, float, true>, attr, sc);
     return e;
 }
 
@@ -323,7 +344,11 @@ void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) 
         using T = decltype(tag);
         const bool vec = a.nx % (16 / (int)sizeof(T)) == 0;
         const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
-        if (mode == TSLB_MODE_COLOUR) {
+        if (mode == TSLB_MODE_COLOUR && a.dtau && std::is_same<T, float>::value) {
+            // per-node tau correction (FP32 storage only; checked by the callers)
+            if (vec) step_kernel<TSLB_MODE_COLOUR, true, float, true><<<grid, block, sm, st>>>(a);
+            else step_kernel<TSLB_MODE_COLOUR, false, float, true><<<grid, block, sm, st>>>(a);
+        } else if (mode == TSLB_MODE_COLOUR) {
             if (vec) step_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, st>>>(a);
             else step_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, st>>>(a);
         } else {
@@ -338,11 +363,16 @@ int launch_step(tslb_ctx* c) {
         int rc = launch_normals(c);
         if (rc) return rc;
     }
+    if (c->closure) {
+        int rc = tslb_internal::closure_before_step(c);
+        if (rc) return rc;
+    }
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
     launch_step_kernel(a, c->p.mode, c->p.precision, c->stream);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
+    c->steps_done++;
     return TSLB_OK;
 }
 
@@ -372,6 +402,10 @@ int state_to_io(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+}  // namespace
+
+namespace tslb_internal {
+
 // FP32 view of the current state: the state itself, or io after conversion
 int fp32_view(tslb_ctx* c, const float** out) {
     if (c->p.precision == TSLB_PREC_FP32) {
@@ -382,6 +416,19 @@ int fp32_view(tslb_ctx* c, const float** out) {
     *out = c->io;
     return rc;
 }
+
+int ensure_dtau(tslb_ctx* c) {
+    if (c->dtau) return TSLB_OK;
+    CUDA_TRY(c, cudaMalloc(&c->dtau, sizeof(float) * c->N));
+    CUDA_TRY(c, cudaMemsetAsync(c->dtau, 0, sizeof(float) * c->N, c->stream));
+    return TSLB_OK;
+}
+
+}  // namespace tslb_internal
+
+namespace {
+
+using tslb_internal::fp32_view;
 
 // Default power-of-two scales of fp16 storage: stored magnitudes near 2^10
 // for typical moments (|rho - 1| < 1/16, |u| < 1/4, |Pi^neq| < 1/16, |phi| <= 1).
@@ -470,6 +517,8 @@ void tslb_destroy(tslb_ctx* c) {
     cudaFree(c->nrm);
     cudaFree(c->flags);
     cudaFree(c->red);
+    cudaFree(c->dtau);
+    cudaFree(c->stats);
     for (int f = 0; f < 6; ++f) cudaFree(c->inlet[f]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -625,6 +674,85 @@ int tslb_set_inlet(tslb_ctx* c, int face, const float* uvw_phi) {
     if (c->p.bc[face] != TSLB_BC_INLET || !c->inlet[face]) return fail(c, TSLB_ERR_ARG, "tslb_set_inlet: face is not an inlet");
     CUDA_TRY(c, cudaMemcpyAsync(c->inlet[face], uvw_phi, sizeof(float) * 4 * face_area(c, face), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return TSLB_OK;
+}
+
+int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
+    if (!c) return TSLB_ERR_ARG;
+    if (c->closure) return fail(c, TSLB_ERR_STATE, "tslb_set_tau_correction: a closure is attached");
+    if (!dtau) {
+        c->dtau_on = false;
+        return TSLB_OK;
+    }
+    if (c->p.mode != TSLB_MODE_COLOUR || c->p.precision != TSLB_PREC_FP32)
+        return fail(c, TSLB_ERR_ARG, "tslb_set_tau_correction: colour mode with FP32 storage only");
+    const float lo = -(std::min(c->p.tau_a, c->p.tau_b) - 0.5f);
+    for (long long i = 0; i < c->n; ++i)
+        if (!std::isfinite(dtau[i]) || !(dtau[i] > lo))
+            return fail(c, TSLB_ERR_ARG, "tslb_set_tau_correction: non-finite value or tau + dtau <= 1/2");
+    int rc = tslb_internal::ensure_dtau(c);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaMemcpyAsync(c->dtau, dtau, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->dtau_on = true;
+    return TSLB_OK;
+}
+
+int tslb_download_tau_correction(tslb_ctx* c, float* dtau) {
+    if (!c || !dtau) return fail(c, TSLB_ERR_ARG, "tslb_download_tau_correction: NULL");
+    if (!c->dtau) {
+        for (long long i = 0; i < c->n; ++i) dtau[i] = 0.f;
+        return TSLB_OK;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(dtau, c->dtau, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return TSLB_OK;
+}
+
+int tslb_stats_reset(tslb_ctx* c) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!c->stats) CUDA_TRY(c, cudaMalloc(&c->stats, sizeof(float) * 5 * c->N));
+    CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, sizeof(float) * 5 * c->N, c->stream));
+    c->stats_count = 0;
+    return TSLB_OK;
+}
+
+int tslb_stats_accumulate(tslb_ctx* c) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "tslb_stats_accumulate before an upload");
+    if (!c->stats) {
+        int rc = tslb_stats_reset(c);
+        if (rc) return rc;
+    }
+    const float* view = nullptr;
+    int rc = fp32_view(c, &view);
+    if (rc) return rc;
+    stats_accumulate_kernel<<<(unsigned)((c->n + 255) / 256), 256, 0, c->stream>>>(view, c->n, c->N, c->stats);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    c->stats_count++;
+    return TSLB_OK;
+}
+
+int tslb_stats_download(tslb_ctx* c, int coarsen, float* u, float* v, float* w, float* phi, float* ww, long long* count) {
+    if (!c) return TSLB_ERR_ARG;
+    if (coarsen < 1 || c->nx % coarsen || c->ny % coarsen || c->nz % coarsen)
+        return fail(c, TSLB_ERR_ARG, "tslb_stats_download: coarsening factor must divide the lattice sizes");
+    if (count) *count = c->stats_count;
+    if (!c->stats || c->stats_count == 0) return fail(c, TSLB_ERR_STATE, "tslb_stats_download: no accumulated samples");
+    const long long nc = c->n / ((long long)coarsen * coarsen * coarsen);
+    float* tmp = nullptr;
+    CUDA_TRY(c, cudaMalloc(&tmp, sizeof(float) * 5 * nc));
+    const float inv = 1.0f / ((float)c->stats_count * coarsen * coarsen * coarsen);
+    stats_coarsen_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(c->stats, c->nx, c->ny, c->nz, c->N, coarsen, inv, tmp);
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    float* dst[5] = {u, v, w, phi, ww};
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+        if (dst[k]) e = cudaMemcpyAsync(dst[k], tmp + k * nc, sizeof(float) * nc, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string("tslb_stats_download: ") + cudaGetErrorString(e));
     return TSLB_OK;
 }
 

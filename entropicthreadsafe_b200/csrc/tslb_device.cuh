@@ -80,6 +80,7 @@ struct StepArgs {
     int wall_phi_mode;
     FaceBC face[6];
     unsigned int* flags;    // bit 0: non-finite moment produced
+    const float* dtau;      // colour: per-node correction of tau (stride N), or null
 };
 
 // Storage types of the moment state: FP32, BF16 or FP16 (scaled).  All
@@ -167,7 +168,7 @@ __device__ float phi_at(const StepArgs& a, int x, int y, int z) {
 }
 
 // normal component `comp` at any node: periodic wrap, zero on solid faces
-__device__ float nrm_at(const StepArgs& a, int comp, int x, int y, int z) {
+__device__ inline float nrm_at(const StepArgs& a, int comp, int x, int y, int z) {
     int c[3] = {x, y, z};
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
@@ -210,7 +211,7 @@ __device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
 }
 
 // -div(n) with the same stencil (recursive_2c_TSLB3D.f90:617-627)
-__device__ float curvature_at(const StepArgs& a, int x, int y, int z) {
+__device__ inline float curvature_at(const StepArgs& a, int x, int y, int z) {
     float div = 0.f;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
@@ -231,8 +232,11 @@ __device__ float curvature_at(const StepArgs& a, int x, int y, int z) {
 
 // Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms.
 // m[] are the node's 11 moments (m[F_D] = rho - 1).
-template <int MODE>
-__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, int x, int y, int z, float* K) {
+// TAU: the node's relaxation time is tau(phi) + dtau[id] (a local eddy-viscosity
+// correction); the surface-tension coefficient follows the corrected omega.
+template <int MODE, bool TAU = false>
+__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, int x, int y, int z, float* K,
+                                           long long id = 0) {
     const float d = m[F_D], rho = 1.f + d;
     const float u = m[F_U], v = m[F_V], w = m[F_W];
     const float pxx = m[F_XX], pxy = m[F_XY], pxz = m[F_XZ], pyy = m[F_YY], pyz = m[F_YZ], pzz = m[F_ZZ];
@@ -248,7 +252,13 @@ __device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, co
         mg = iface ? m2 * rs : 0.f;
         // 1/nu = (rhoA/rho)/nu_a + (rhoB/rho)/nu_b ; omega = 2/(6 nu + 1) = 2q/(6 + q)
         const float q = 0.5f * ((a.inv_nu_a + a.inv_nu_b) + phi * (a.inv_nu_a - a.inv_nu_b));
-        omega = __fdividef(2.f * q, 6.f + q);
+        if (TAU) {
+            // 1/omega = (6 + q)/(2q) + dtau
+            const float dt = __ldg(a.dtau + id);
+            omega = __fdividef(2.f * q, fmaf(2.f * q, dt, 6.f + q));
+        } else {
+            omega = __fdividef(2.f * q, 6.f + q);
+        }
         // branch-free: outside the interface A = 0 and n = 0
         const float inv = iface ? rs : 0.f;
         nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;

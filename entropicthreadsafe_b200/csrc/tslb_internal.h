@@ -1,0 +1,55 @@
+// tslb_internal.h -- the lattice context shared by the translation units of
+// libtslb.so (tslb.cu: step and diagnostics; closure.cu: the learned
+// eddy-viscosity closure).  Not part of the C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/tslb.h"
+#include "tslb_device.cuh"
+
+struct tslb_closure;
+
+struct tslb_ctx {
+    tslb_params p;
+    int nx, ny, nz;
+    long long n;        // nodes
+    long long N;        // padded field stride
+    int device;
+    cudaStream_t stream = nullptr;
+    void* state[2] = {nullptr, nullptr};   // ping-pong, 11 fields each, storage type
+    int esize = 4;                         // bytes per stored element
+    float* io = nullptr;                   // FP32 conversion buffer (bf16/fp16 storage)
+    float scale[tslb::NF];                 // fp16 storage: stored = value * scale
+    int cur = 0;
+    float* nrm = nullptr;                  // 3 fields
+    float* inlet[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    unsigned int* flags = nullptr;
+    double* red = nullptr;                 // reduction accumulators
+    bool loaded = false;
+    int zchunk = 32;
+    long long launches = 0;
+    // per-node tau correction (colour mode, FP32 storage): read by the step
+    // kernel when dtau_on; written by tslb_set_tau_correction or the closure
+    float* dtau = nullptr;
+    bool dtau_on = false;
+    tslb_closure* closure = nullptr;       // attached closure (not owned)
+    int closure_interval = 1;
+    long long steps_done = 0;
+    // running sums of u, v, w, phi, w^2 (tslb_stats_*)
+    float* stats = nullptr;
+    long long stats_count = 0;
+    std::string err;
+};
+
+namespace tslb_internal {
+// record msg as the context's (or, for ctx == NULL, the creation) error; returns code
+int fail(tslb_ctx* c, int code, const std::string& msg);
+// FP32 view of the current state (converted through io for bf16/fp16 storage)
+int fp32_view(tslb_ctx* c, const float** out);
+// allocate the per-node tau correction buffer (zeroed) if absent
+int ensure_dtau(tslb_ctx* c);
+// closure.cu: refresh c->dtau from the attached closure before a step
+int closure_before_step(tslb_ctx* c);
+}  // namespace tslb_internal

@@ -149,7 +149,7 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 
 // Regularized or bounce-back populations entering target (x,y,z) from
 // behind non-periodic faces; Kp points at the target's own coefficients.
-template <int MODE, class T>
+template <int MODE, class T, bool TAU = false>
 __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y, int z,
                                 float* acc) {
     float Kp[NCOEF];
@@ -234,7 +234,8 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             if (MODE == TSLB_MODE_COLOUR) {
                 const float ca = 0.5f * (1.f + m[F_PHI]), cb = 0.5f * (1.f - m[F_PHI]);
                 const float nu = 1.f / (ca * a.inv_nu_a + cb * a.inv_nu_b);
-                omega = 2.f / (6.f * nu + 1.f);
+                const float dt = TAU ? __ldg(a.dtau + nidx(a, x, y, z)) : 0.f;
+                omega = 2.f / (6.f * nu + 1.f + 2.f * dt);
             } else {
                 omega = a.omega_pf;
             }
@@ -362,7 +363,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // VEC: nx is a multiple of the 16-byte chunk, so chunks never straddle the
 // x faces and planes are staged with 16-byte cp.async copies.
 // One block's work: tile (bx, by) of columns and z chunk bz of lattice a.
-template <int MODE, bool VEC, class T>
+template <int MODE, bool VEC, class T, bool TAU = false>
 __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, int bz) {
     using G = Geo<sizeof(T)>;
     constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
@@ -570,7 +571,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                     gx = nd.off % a.nx;
                     gy = nd.off / a.nx;
                 }
-                node_coefs<MODE>(a, m, g, gx, gy, gz, K);
+                node_coefs<MODE, TAU>(a, m, g, gx, gy, gz, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs(coef + ci, K);
         }
@@ -597,7 +598,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 unsigned mask = colmask;
                 if (!zper && s == 0) mask |= 16u;
                 if (!zper && s == a.nz - 1) mask |= 32u;
-                if (mask) boundary_target<MODE, T>(a, Kc, mask, X, Y, s, acc0);
+                if (mask) boundary_target<MODE, T, TAU>(a, Kc, mask, X, Y, s, acc0);
             }
             // ---- 4. target plane s-1 is complete ----
             const int t = s - 1;
@@ -635,9 +636,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     cp_async_wait<0>();
 }
 
-template <int MODE, bool VEC, class T>
+template <int MODE, bool VEC, class T, bool TAU = false>
 __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
-    step_block<MODE, VEC, T>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+    step_block<MODE, VEC, T, TAU>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Work item of the ensemble kernel: lattice, tile column, z chunk.

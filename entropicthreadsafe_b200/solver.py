@@ -82,6 +82,37 @@ class Lattice:
         planes = np.ascontiguousarray(planes, np.float32)
         self._check(self.L.tslb_set_inlet(self.h, face, capi.fptr(planes)))
 
+    def set_tau_correction(self, dtau) -> None:
+        """Per-node relaxation-time correction (nz, ny, nx), or None to switch it off."""
+        if dtau is None:
+            self._check(self.L.tslb_set_tau_correction(self.h, None))
+            return
+        d = np.ascontiguousarray(dtau, np.float32).reshape(self.shape)
+        self._check(self.L.tslb_set_tau_correction(self.h, capi.fptr(d)))
+
+    def tau_correction(self) -> np.ndarray:
+        out = np.empty(self.shape, np.float32)
+        self._check(self.L.tslb_download_tau_correction(self.h, capi.fptr(out)))
+        return out
+
+    # -- time averages ---------------------------------------------------
+    def stats_reset(self) -> None:
+        self._check(self.L.tslb_stats_reset(self.h))
+
+    def stats_accumulate(self) -> None:
+        self._check(self.L.tslb_stats_accumulate(self.h))
+
+    def stats(self, coarsen: int = 1) -> dict:
+        """Means of u, v, w, phi, w^2 over the accumulated samples, averaged over coarsen^3 blocks."""
+        nz, ny, nx = self.shape
+        shp = (nz // coarsen, ny // coarsen, nx // coarsen)
+        out = {k: np.empty(shp, np.float32) for k in ("u", "v", "w", "phi", "ww")}
+        cnt = ctypes.c_longlong()
+        self._check(self.L.tslb_stats_download(self.h, coarsen, *[capi.fptr(out[k]) for k in ("u", "v", "w", "phi", "ww")],
+                                               ctypes.byref(cnt)))
+        out["count"] = int(cnt.value)
+        return out
+
     # -- time stepping ---------------------------------------------------
     def step(self, nsteps: int = 1) -> None:
         self._check(self.L.tslb_step(self.h, nsteps))

@@ -164,6 +164,30 @@ int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
  * four planes (u, v, w, phi) of the face's extent, Fortran order. */
 int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
 
+/* Per-node correction dtau of the relaxation time (colour mode, FP32
+ * storage): node x relaxes with tau(phi_x) + dtau[x], i.e. an added local
+ * viscosity dtau/3, in the collision and in the regularized faces; the
+ * surface-tension coefficient follows the corrected omega.  dtau holds
+ * nx*ny*nz values (Fortran order) with tau + dtau > 1/2; NULL switches the
+ * correction off.  The reference has no counterpart: it is the hook of the
+ * learned eddy-viscosity closure (tslb_closure.h), which writes the same
+ * buffer on the device. */
+int  tslb_set_tau_correction(tslb_ctx* ctx, const float* dtau);
+/* The current correction (zeros when none was set). */
+int  tslb_download_tau_correction(tslb_ctx* ctx, float* dtau);
+
+/* Time averages on the device: tslb_stats_accumulate adds u, v, w, phi and
+ * w^2 of the current state to running sums (asynchronous);
+ * tslb_stats_download returns their means over the accumulated samples,
+ * averaged over coarsen^3 blocks (coarsen divides nx, ny, nz; outputs have
+ * (nx/coarsen)*(ny/coarsen)*(nz/coarsen) values; any pointer may be NULL)
+ * and the sample count.  They stand in for the host-side averaging the
+ * reference's drivers do on frames written by print_module.f90. */
+int  tslb_stats_reset(tslb_ctx* ctx);
+int  tslb_stats_accumulate(tslb_ctx* ctx);
+int  tslb_stats_download(tslb_ctx* ctx, int coarsen, float* u, float* v, float* w, float* phi, float* ww,
+                         long long* count);
+
 /* Wait for all work queued on the context stream. */
 int  tslb_synchronize(tslb_ctx* ctx);
 

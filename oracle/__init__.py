@@ -49,6 +49,8 @@ def _lib(fast: bool = False) -> ctypes.CDLL:
         lib.orc_set_pops.restype = ip
         lib.orc_set_inlet.argtypes = [vp, ip, dp]
         lib.orc_set_inlet.restype = ip
+        lib.orc_set_dtau.argtypes = [vp, dp]
+        lib.orc_set_dtau.restype = ip
         lib.orc_step.argtypes = [vp, ip]
         lib.orc_step.restype = ip
         _LIBS[name] = lib
@@ -110,6 +112,14 @@ class Oracle:
     def set_inlet(self, face: int, planes: np.ndarray) -> None:
         planes = np.ascontiguousarray(planes, np.float64)
         self._check(self.lib.orc_set_inlet(self.h, face, _dptr(planes)))
+
+    def set_tau_correction(self, dtau) -> None:
+        """Per-node correction of the colour-mode relaxation time, (nz, ny, nx), or None."""
+        if dtau is None:
+            self._check(self.lib.orc_set_dtau(self.h, None))
+            return
+        d = np.ascontiguousarray(dtau, np.float64).reshape(self.shape)
+        self._check(self.lib.orc_set_dtau(self.h, _dptr(d)))
 
     def normals(self) -> np.ndarray:
         buf = np.empty((3,) + self.shape, np.float64)

@@ -71,6 +71,15 @@ int set_inlet_t(orc::Oracle<R>& o, int face, const double* in) {
     return TSLB_OK;
 }
 
+template <class R>
+int set_dtau_t(orc::Oracle<R>& o, const double* in) {
+    size_t n = size_t(o.nx) * o.ny * o.nz;
+    if (!in) { o.dtau.clear(); return TSLB_OK; }
+    o.dtau.resize(n);
+    for (size_t s = 0; s < n; ++s) o.dtau[s] = R(in[s]);
+    return TSLB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -100,6 +109,7 @@ int orc_set_inlet(void* hp, int face, const double* in) {
     if (face < 0 || face > 5) return TSLB_ERR_ARG;
     ORC_DISPATCH(hp, set_inlet_t(o, face, in));
 }
+int orc_set_dtau(void* hp, const double* in) { ORC_DISPATCH(hp, set_dtau_t(o, in)); }
 int orc_step(void* hp, int nsteps) {
     ORC_DISPATCH(hp, (([&]() { for (int s = 0; s < nsteps; ++s) o.step(); return int(TSLB_OK); })()));
 }

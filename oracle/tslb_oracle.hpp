@@ -170,6 +170,16 @@ struct Oracle {
     R& G(int q, int i, int j, int k) { return g[size_t(q) * vol + id(i, j, k)]; }
     R omega_pf() const { return R(1) / R(prm.tau_a); }
 
+    // per-node correction of the colour-mode relaxation time (empty: none);
+    // the B200 path's tslb_set_tau_correction and learned closure
+    std::vector<R> dtau;
+    R node_dtau(int i, int j, int k) const { return dtau.empty() ? R(0) : dtau[iid(i, j, k)]; }
+    // omega = 1/tau with tau = 3 nu + 1/2 (+ dtau)
+    R omega_colour(R nu, int i, int j, int k) const {
+        if (dtau.empty()) return R(2) / (R(6) * nu + R(1));
+        return R(1) / (R(3) * nu + R(0.5) + node_dtau(i, j, k));
+    }
+
     // inlet plane value of face fc at the in-plane coordinates of node (i,j,k)
     size_t plane_index(int fc, int i, int j, int k) const {
         int a = fc / 2;
@@ -396,7 +406,8 @@ struct Oracle {
                     const R m2 = gp[0] * gp[0] + gp[1] * gp[1] + gp[2] * gp[2];
                     const R m = std::sqrt(m2);
                     const R nu = R(1) / (ca / nu_a + cb / nu_b);
-                    const R omega = R(2) / (R(6) * nu + R(1));
+                    // tau = 3 nu + 1/2, plus the per-node correction when set
+                    const R omega = omega_colour(nu, i, j, k);
                     const R A = colour_surface_coeff() * sigma * omega;
                     const bool iface = m > thr;
                     const R rec = beta * ca * cb * rho;  // beta rhoA rhoB / rho
@@ -461,7 +472,7 @@ struct Oracle {
             const R nu_a = (R(prm.tau_a) - R(0.5)) / R(3), nu_b = (R(prm.tau_b) - R(0.5)) / R(3);
             const R ca = (R(1) + phi) / R(2), cb = (R(1) - phi) / R(2);
             const R nu = R(1) / (ca / nu_a + cb / nu_b);
-            omega = R(2) / (R(6) * nu + R(1));
+            omega = omega_colour(nu, i, j, k);
         } else {
             omega = omega_pf();
         }

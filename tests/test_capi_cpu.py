@@ -8,14 +8,18 @@ import pytest
 
 from entropicthreadsafe_b200 import capi
 
-HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "tslb.h")
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+HEADERS = ("tslb.h", "tslb_closure.h")
 
 
 def declared_symbols():
-    with open(HEADER) as fh:
-        text = fh.read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(tslb_[a-z_0-9]+)\s*\(", text)))
+    names = set()
+    for h in HEADERS:
+        with open(os.path.join(INCLUDE, h)) as fh:
+            text = fh.read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(tslb_[a-z_0-9]+)\s*\(", text))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -27,7 +31,8 @@ def lib():
 
 def test_library_exports_every_declared_symbol(lib):
     names = declared_symbols()
-    assert len(names) >= 12
+    assert len(names) >= 40
+    assert "tslb_closure_train" in names and "tslb_set_tau_correction" in names
     for name in names:
         assert hasattr(lib, name), name
 
