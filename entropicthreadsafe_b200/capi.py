@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libtslb.so")
 OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(7)
 MODE_PHASEFIELD, MODE_COLOUR = 0, 1
 PREC_FP32, PREC_BF16, PREC_FP16S = 0, 1, 2
-BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET = range(5)
+BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET, BC_PRESSURE = range(6)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
 NREDUCE = 12
 NOALLOC_MAX_NODES = 1 << 20
@@ -106,7 +106,7 @@ def _declare_closure(L) -> None:
         "tslb_closure_gradient": ([vp, fp, fp, fp, ll, fp, dp], ip),
         "tslb_closure_dataset_clear": ([vp], ip),
         "tslb_closure_dataset_add": ([vp, fp, fp, fp, ll], ip),
-        "tslb_closure_dataset_add_fine": ([vp, vp, ctypes.c_float, ip, ctypes.POINTER(ll)], ip),
+        "tslb_closure_dataset_add_fine": ([vp, vp, ctypes.c_float, ip, ip, ip, ctypes.POINTER(ll)], ip),
         "tslb_closure_dataset_size": ([vp], ll),
         "tslb_closure_dataset_download": ([vp, fp, fp, fp], ip),
         "tslb_closure_normalize": ([vp], ip),
@@ -187,6 +187,8 @@ def lib() -> ctypes.CDLL:
         L.tslb_ensemble_last_error.argtypes = [vp]
         L.tslb_ensemble_last_error.restype = ctypes.c_char_p
         lp = ctypes.POINTER(ctypes.c_longlong)
+        L.tslb_set_inlet_disc.argtypes = [vp, ip] + [ctypes.c_float] * 5 + [ctypes.c_ulonglong] * 2
+        L.tslb_set_inlet_disc.restype = ip
         L.tslb_set_tau_correction.argtypes = [vp, fp]
         L.tslb_set_tau_correction.restype = ip
         L.tslb_download_tau_correction.argtypes = [vp, fp]

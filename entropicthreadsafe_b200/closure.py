@@ -140,9 +140,11 @@ class Closure:
         w = np.ascontiguousarray(weight, np.float32).reshape(-1)
         self._check(self.L.tslb_closure_dataset_add(self.h, capi.fptr(f), capi.fptr(t), capi.fptr(w), f.shape[0]))
 
-    def dataset_add_fine(self, fine: Lattice, pi_scale: float, keep_every: int = 1) -> int:
+    def dataset_add_fine(self, fine: Lattice, pi_scale: float, keep_every: int = 1, z_range=(0, 0)) -> int:
+        """Samples of the fine lattice on the coarse planes z_range[0] <= z < z_range[1] (0: to the end)."""
         n = ctypes.c_longlong()
-        self._check(self.L.tslb_closure_dataset_add_fine(self.h, fine.h, float(pi_scale), int(keep_every), ctypes.byref(n)))
+        self._check(self.L.tslb_closure_dataset_add_fine(self.h, fine.h, float(pi_scale), int(keep_every),
+                                                         int(z_range[0]), int(z_range[1]), ctypes.byref(n)))
         return int(n.value)
 
     @property

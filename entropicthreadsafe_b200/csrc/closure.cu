@@ -26,6 +26,7 @@ using tslb::F_XX;
 struct tslb_closure {
     int device = 0;
     int sms = 148;
+    int infer_per_sm = 1, train_per_sm = 1;   // resident CTAs per SM (occupancy API)
     cudaStream_t stream = nullptr;
     float* params = nullptr;   // FP32 master, NPARAM_PAD
     float* adam_m = nullptr;
@@ -52,11 +53,12 @@ static std::string g_closure_create_error;
 namespace {
 
 constexpr int TRAIN_SMEM = 104 * 1024;   // caps residency at 2 CTAs/SM (256 TMEM columns each)
-constexpr int INFER_SMEM = 56 * 1024;    // caps residency at 4 CTAs/SM (128 TMEM columns each)
 constexpr int OFF_ACT = IMG_BYTES, OFF_DZ = IMG_BYTES + ACT_BYTES;
-constexpr int OFF_MISC_TRAIN = OFF_DZ + DZ_BYTES, OFF_MISC_INFER = OFF_ACT + ACT_BYTES;
+constexpr int OFF_MISC_TRAIN = OFF_DZ + DZ_BYTES, OFF_MISC_INFER = OFF_ACT + Act<NCH_INFER>::BYTES;
+// image + 10-chunk ACT + barrier words: at most 7 CTAs/SM (64 TMEM columns each)
+constexpr int INFER_SMEM = OFF_MISC_INFER + 64;
 static_assert(OFF_MISC_TRAIN + 2048 + 32 * 1024 <= TRAIN_SMEM, "training tail space");
-static_assert(OFF_MISC_INFER + 256 <= INFER_SMEM, "inference shared memory");
+static_assert(8 * (INFER_SMEM + 1024) > 228 * 1024 && 7 * 64 <= 512, "inference residency vs TMEM columns");
 
 int cfail(tslb_closure* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -80,9 +82,10 @@ __global__ void image_kernel(const float* __restrict__ params, Image* img) {
     __nv_bfloat16* w2 = reinterpret_cast<__nv_bfloat16*>(img->w2);
     if (p < P_B1) {
         const int n = p / KIN, k = p % KIN;
-        w1[w1_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(k < NFEAT ? v : 0.f);
+        if (k != NFEAT) w1[w1_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(k < NFEAT ? v : 0.f);
     } else if (p < P_W2) {
         img->b1[p - P_B1] = v;
+        w1[w1_chunk(p - P_B1, 1) * 8 + (NFEAT & 7)] = __float2bfloat16_rn(v);   // bias column
     } else if (p < P_B2) {
         const int n = (p - P_W2) / NH, k = (p - P_W2) % NH;
         w2[w2_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(v);
@@ -153,11 +156,19 @@ struct ArraySrc {
     const float* feat;
     float* out;
     long long n;
-    __device__ bool features(long long i, float* f) const {
+    struct Raw {
+        float f[NFEAT];
+    };
+    __device__ void load(long long i, Raw& r) const {
+        if (i >= n) return;
+#pragma unroll
+        for (int k = 0; k < NFEAT; ++k) r.f[k] = feat[i * NFEAT + k];
+    }
+    __device__ bool features(const Raw& r, long long, float* f) const {
         bool ok = true;
 #pragma unroll
         for (int k = 0; k < NFEAT; ++k) {
-            f[k] = feat[i * NFEAT + k];
+            f[k] = r.f[k];
             ok = ok && isfinite(f[k]);
         }
         return ok;
@@ -173,75 +184,99 @@ struct LatticeSrc {
     int nx, ny, nz;
     int px, py, pz;
     float inv_nu_a, inv_nu_b;
-    float* dtau;
+    float* dtau;         // total correction of the previous refresh, rewritten (null: none)
+    const float* base;   // static correction (tslb_set_tau_correction) or null
+    struct Raw {
+        float P[6], phi, u, v, w, ph[6], dprev;
+    };
     __device__ float phi_at(int x, int y, int z) const {
         return st[F_PHI * N + x + (long long)nx * (y + (long long)ny * z)];
     }
-    __device__ bool features(long long i, float* f) const {
-        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
-        float P[6];
+    __device__ void load(long long i, Raw& r) const {
+        if (i >= n) return;
+        int x, y, z;
+        if (n < (1LL << 31)) {
+            const int ii = (int)i, q = ii / nx;
+            x = ii - q * nx;
+            z = q / ny;
+            y = q - z * ny;
+        } else {
+            x = (int)(i % nx); y = (int)((i / nx) % ny); z = (int)(i / ((long long)nx * ny));
+        }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) P[k] = st[(F_XX + k) * N + i];
-        const float phi = st[F_PHI * N + i];
-        const float u = st[F_U * N + i], v = st[F_V * N + i], w = st[F_W * N + i];
-        const float gx = 0.5f * (phi_at(nbr(x, 1, nx, px), y, z) - phi_at(nbr(x, -1, nx, px), y, z));
-        const float gy = 0.5f * (phi_at(x, nbr(y, 1, ny, py), z) - phi_at(x, nbr(y, -1, ny, py), z));
-        const float gz = 0.5f * (phi_at(x, y, nbr(z, 1, nz, pz)) - phi_at(x, y, nbr(z, -1, nz, pz)));
+        for (int k = 0; k < 6; ++k) r.P[k] = st[(F_XX + k) * N + i];
+        r.phi = st[F_PHI * N + i];
+        r.u = st[F_U * N + i]; r.v = st[F_V * N + i]; r.w = st[F_W * N + i];
+        r.ph[0] = phi_at(nbr(x, 1, nx, px), y, z);
+        r.ph[1] = phi_at(nbr(x, -1, nx, px), y, z);
+        r.ph[2] = phi_at(x, nbr(y, 1, ny, py), z);
+        r.ph[3] = phi_at(x, nbr(y, -1, ny, py), z);
+        r.ph[4] = phi_at(x, y, nbr(z, 1, nz, pz));
+        r.ph[5] = phi_at(x, y, nbr(z, -1, nz, pz));
+        r.dprev = dtau ? dtau[i] : 0.f;
+    }
+    __device__ bool features(const Raw& r, long long, float* f) const {
+        const float gx = 0.5f * (r.ph[0] - r.ph[1]), gy = 0.5f * (r.ph[2] - r.ph[3]), gz = 0.5f * (r.ph[4] - r.ph[5]);
         // plain tau of the node's mixture: 1/omega = (6 + q)/(2q)
-        const float q = 0.5f * ((inv_nu_a + inv_nu_b) + phi * (inv_nu_a - inv_nu_b));
+        const float q = 0.5f * ((inv_nu_a + inv_nu_b) + r.phi * (inv_nu_a - inv_nu_b));
         const float tau = (6.f + q) / (2.f * q);
-        const float s = tau / (tau + dtau[i]);
-        make_features(s, P, phi, sqrtf(gx * gx + gy * gy + gz * gz), sqrtf(u * u + v * v + w * w), f);
+        const float s = tau / (tau + r.dprev);
+        make_features(s, r.P, r.phi, sqrtf(gx * gx + gy * gy + gz * gz), sqrtf(r.u * r.u + r.v * r.v + r.w * r.w), f);
         bool ok = true;
 #pragma unroll
         for (int k = 0; k < NFEAT; ++k) ok = ok && isfinite(f[k]);
         return ok;
     }
-    __device__ void store(long long i, float y) const { dtau[i] = y; }
+    __device__ void store(long long i, float y) const { dtau[i] = base ? y + base[i] : y; }
 };
 
 // Inference: dtau = dtau_max sigmoid(o) for every row of the source, 128
-// rows per tile, tiles strided over a persistent grid.
+// rows per tile, tiles strided over a persistent grid.  The next tile's
+// inputs are loaded while this tile's MMAs run; both layers accumulate in
+// the same 64 TMEM columns, so up to 7 CTAs share an SM.
 template <class Src>
-__global__ void __launch_bounds__(TILE, 1) infer_kernel(const Image* __restrict__ gimg, Src src, long long n,
+__global__ void __launch_bounds__(TILE, 6) infer_kernel(const Image* __restrict__ gimg, Src src, long long n,
                                                         unsigned int* gflag) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    Smem S = smem_setup(sm, gimg, OFF_MISC_INFER, false, 128);
+    Smem S = smem_setup(sm, gimg, OFF_MISC_INFER, false, 64);
     const uint32_t tb = *S.tslot;
     const Image& im = *S.im;
     const int tid = threadIdx.x;
     const uint32_t act_a = tc::smem_u32(S.act), w1_a = tc::smem_u32(im.w1), w2_a = tc::smem_u32(im.w2);
     uint32_t ph = 0;
     const long long ntiles = (n + TILE - 1) / TILE;
+    typename Src::Raw raw;
+    if ((long long)blockIdx.x < ntiles) src.load((long long)blockIdx.x * TILE + tid, raw);
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const long long i = t * TILE + tid;
         const bool valid = i < n;
         float f[NFEAT];
-        const bool fin = valid && src.features(i, f);
-        put_x(S.act, tid, f, im, fin);
+        const bool fin = valid && src.features(raw, i, f);
+        if (t + gridDim.x < ntiles) src.load((t + gridDim.x) * TILE + tid, raw);
+        put_x<NCH_INFER>(S.act, tid, f, im, fin);
         sync_for_mma();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_fwd1(tb, act_a, w1_a);
+            issue_fwd1<NCH_INFER>(tb, act_a, w1_a, 0);
             tc::mma_commit(S.bar);
         }
         if (!wait_mma(S.bar, ph, S.abort_s, gflag)) break;
-        epi_h1(tb, S.act, tid, im);
+        epi_h1<NCH_INFER, false>(tb, S.act, tid, 0);
         sync_for_mma();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_fwd2(tb, act_a, w2_a);
+            issue_fwd2<NCH_INFER>(tb, act_a, w2_a, 0);
             tc::mma_commit(S.bar);
         }
         if (!wait_mma(S.bar, ph, S.abort_s, gflag)) break;
-        const float o = epi_out(tb, im);
+        const float o = epi_out(tb, im, 0);
         float y = im.dtau_max / (1.f + expf(-o));
         // stability clamp: the plain tau where anything is not finite
         if (!fin || !isfinite(y)) y = 0.f;
         y = fminf(fmaxf(y, 0.f), im.dtau_max);
         if (valid) src.store(i, y);
     }
-    smem_teardown(S, tb, 128, ph);
+    smem_teardown(S, tb, 64, ph);
 }
 
 struct TrainArgs {
@@ -303,7 +338,7 @@ __global__ void __launch_bounds__(TILE, 1) train_kernel(const TrainArgs a) {
             tc::mma_commit(S.bar);
         }
         if (!wait_mma(S.bar, ph, S.abort_s, a.flags)) break;
-        const uint64_t m1 = epi_h1(tb, S.act, tid, im);
+        const uint64_t m1 = epi_h1<NCH_TRAIN, true>(tb, S.act, tid, COL_Z1);
         sync_for_mma();
         if (tid == 0) {
             tc::fence_after_sync();
@@ -342,16 +377,16 @@ __global__ void __launch_bounds__(TILE, 1) train_kernel(const TrainArgs a) {
     const int row = 32 * warp + lane;
     const bool have = !first && *S.abort_s == 0;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        float d[16];
-        if (have) tc::tmem_ld16(lane_addr(tb, COL_DW + 16 * q), d);
+    for (int q = 0; q < 3; ++q) {
+        float d[32];
+        if (have) tc::tmem_ld32(lane_addr(tb, COL_DW + 32 * q), d);
         else {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) d[j] = 0.f;
+            for (int j = 0; j < 32; ++j) d[j] = 0.f;
         }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int col = 16 * q + j;
+        for (int j = 0; j < 32; ++j) {
+            const int col = 32 * q + j;
             if (row < NH) {
                 if (col < NH) part[P_W2 + row * NH + col] = d[j];
                 else if (col == 80) part[P_B2 + row] = d[j];
@@ -419,9 +454,10 @@ __global__ void adam_kernel(const AdamArgs a) {
     __nv_bfloat16* w2 = reinterpret_cast<__nv_bfloat16*>(a.img->w2);
     if (p < P_B1) {
         const int n = p / KIN, k = p % KIN;
-        w1[w1_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(w);
+        if (k != NFEAT) w1[w1_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(w);
     } else if (p < P_W2) {
         a.img->b1[p - P_B1] = w;
+        w1[w1_chunk(p - P_B1, 1) * 8 + (NFEAT & 7)] = __float2bfloat16_rn(w);   // bias column
     } else if (p < P_B2) {
         const int n = (p - P_W2) / NH, k = (p - P_W2) % NH;
         w2[w2_chunk(n, k >> 3) * 8 + (k & 7)] = __float2bfloat16_rn(w);
@@ -468,12 +504,12 @@ __global__ void coarsen_kernel(const float* __restrict__ st, long long N, int nx
 // t = 3 nu_t = -3 (tau_dev : S)/(2 S : S) and weight a = S : S (0 on
 // non-periodic boundary planes, where the differences are one-sided)
 __global__ void samples_kernel(const float* __restrict__ inter, int cx, int cy, int cz, int px, int py, int pz, int keep,
-                               int phase, long long base, float* __restrict__ feat, float* __restrict__ tgt,
-                               float* __restrict__ wgt) {
+                               long long J0, long long J1, long long base, float* __restrict__ feat,
+                               float* __restrict__ tgt, float* __restrict__ wgt) {
     const long long nc = (long long)cx * cy * cz;
     const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long J = phase + r * keep;
-    if (J >= nc) return;
+    const long long J = J0 + r * keep;
+    if (J >= J1) return;
     const int X = (int)(J % cx), Y = (int)((J / cx) % cy), Z = (int)(J / ((long long)cx * cy));
     auto at = [&](int k, int x, int y, int z) { return inter[k * nc + x + (long long)cx * (y + (long long)cy * z)]; };
     const int xp = nbr(X, 1, cx, px), xm = nbr(X, -1, cx, px);
@@ -551,19 +587,47 @@ __global__ void features_kernel(LatticeSrc src, float* __restrict__ out) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= src.n) return;
     float f[NFEAT];
-    src.features(i, f);
+    LatticeSrc::Raw r;
+    src.load(i, r);
+    src.features(r, i, f);
 #pragma unroll
     for (int k = 0; k < NFEAT; ++k) out[i * NFEAT + k] = f[k];
 }
 
 // ------------------------------------------------------------ host helpers
 cudaError_t set_attributes() {
-    cudaError_t e = cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TRAIN_SMEM);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(infer_kernel<ArraySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize, INFER_SMEM);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(infer_kernel<LatticeSrc>, cudaFuncAttributeMaxDynamicSharedMemorySize, INFER_SMEM);
+    const cudaFuncAttribute dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    const cudaFuncAttribute carve = cudaFuncAttributePreferredSharedMemoryCarveout;
+    cudaError_t e = cudaFuncSetAttribute(train_kernel, dyn, TRAIN_SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(infer_kernel<ArraySrc>, dyn, INFER_SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(infer_kernel<LatticeSrc>, dyn, INFER_SMEM);
+    // all of the unified L1/shared storage as shared memory, so residency is set by the
+    // kernels' shared memory and registers (and the occupancy query agrees with the launch)
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(train_kernel, carve, (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(infer_kernel<ArraySrc>, carve, (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(infer_kernel<LatticeSrc>, carve, (int)cudaSharedmemCarveoutMaxShared);
     return e;
+}
+
+// CTAs of TILE threads that fit on one SM by registers (allocated per warp
+// in units of 8 per thread), shared memory (plus the per-block reserve) and
+// threads.  The runtime's occupancy query under-reports for these kernels.
+cudaError_t resident_ctas(int dev, const void* fn, int smem, int* out) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    int regs_sm = 65536, smem_sm = 233472, reserve = 1024, thr_sm = 2048;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    const int regs_warp = ((fa.numRegs + 7) / 8) * 8 * 32;
+    const int warps = TILE / 32;
+    int n = regs_sm / (regs_warp * warps);
+    n = std::min(n, smem_sm / (smem + (int)fa.sharedSizeBytes + reserve));
+    n = std::min(n, thr_sm / TILE);
+    *out = std::max(n, 1);
+    return cudaSuccess;
 }
 
 int upload_meta(tslb_closure* c) {
@@ -611,7 +675,7 @@ int ensure_partial(tslb_closure* c, int nctas) {
 int train_pass(tslb_closure* c, const float* feat, const float* tgt, const float* wgt, long long ndata, long long nrows,
                int random, unsigned long long seed, int step, float lr, float* grad_out, float* loss_out) {
     const long long ntiles = (nrows + TILE - 1) / TILE;
-    const int grid = (int)std::min<long long>(ntiles, 2LL * c->sms);
+    const int grid = (int)std::min<long long>(ntiles, (long long)c->train_per_sm * c->sms);
     int rc = ensure_partial(c, grid);
     if (rc) return rc;
     TrainArgs a;
@@ -644,6 +708,7 @@ LatticeSrc lattice_src(tslb_ctx* L, const float* view) {
     s.inv_nu_a = 3.0f / (L->p.tau_a - 0.5f);
     s.inv_nu_b = 3.0f / (L->p.tau_b - 0.5f);
     s.dtau = L->dtau;
+    s.base = L->base_on ? L->dtau_base : nullptr;
     return s;
 }
 
@@ -683,7 +748,7 @@ int closure_before_step(tslb_ctx* L) {
     int rc = fp32_view(L, &view);
     if (rc) return rc;
     const long long ntiles = (L->n + TILE - 1) / TILE;
-    const int grid = (int)std::min<long long>(ntiles, 4LL * c->sms);
+    const int grid = (int)std::min<long long>(ntiles, (long long)c->infer_per_sm * c->sms);
     infer_kernel<LatticeSrc><<<grid, TILE, INFER_SMEM, L->stream>>>(c->img, lattice_src(L, view), L->n, L->flags);
     L->launches++;
     cudaError_t e = cudaGetLastError();
@@ -723,6 +788,11 @@ int tslb_closure_create(tslb_closure** out) {
     cudaMemset(c->flags, 0, sizeof(unsigned int));
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(e, "cudaMemset");
     if ((e = set_attributes()) != cudaSuccess) return bail(e, "cudaFuncSetAttribute");
+    // persistent grids: exactly the CTAs that can be resident at once
+    if ((e = resident_ctas(c->device, (const void*)infer_kernel<LatticeSrc>, INFER_SMEM, &c->infer_per_sm)) != cudaSuccess)
+        return bail(e, "resident_ctas");
+    if ((e = resident_ctas(c->device, (const void*)train_kernel, TRAIN_SMEM, &c->train_per_sm)) != cudaSuccess)
+        return bail(e, "resident_ctas");
     if (rebuild_image(c) || upload_meta(c)) {
         g_closure_create_error = c->err;
         tslb_closure_destroy(c);
@@ -794,7 +864,7 @@ int tslb_closure_forward(tslb_closure* c, const float* features, long long n, fl
     CL_TRY(c, cudaMemcpyAsync(d.f, features, sizeof(float) * NFEAT * n, cudaMemcpyHostToDevice, c->stream));
     ArraySrc src{d.f, d.y, n};
     const long long ntiles = (n + TILE - 1) / TILE;
-    const int grid = (int)std::min<long long>(ntiles, 4LL * c->sms);
+    const int grid = (int)std::min<long long>(ntiles, (long long)c->infer_per_sm * c->sms);
     infer_kernel<ArraySrc><<<grid, TILE, INFER_SMEM, c->stream>>>(c->img, src, n, c->flags);
     CL_TRY(c, cudaGetLastError());
     CL_TRY(c, cudaMemcpyAsync(dtau, d.y, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
@@ -844,7 +914,8 @@ int tslb_closure_dataset_add(tslb_closure* c, const float* features, const float
     return TSLB_OK;
 }
 
-int tslb_closure_dataset_add_fine(tslb_closure* c, tslb_ctx* fine, float pi_scale, int keep_every, long long* added) {
+int tslb_closure_dataset_add_fine(tslb_closure* c, tslb_ctx* fine, float pi_scale, int keep_every, int z_lo, int z_hi,
+                                  long long* added) {
     if (!c || !fine) return cfail(c, TSLB_ERR_ARG, "tslb_closure_dataset_add_fine: NULL");
     if (added) *added = 0;
     if (fine->p.mode != TSLB_MODE_COLOUR) return cfail(c, TSLB_ERR_ARG, "the fine lattice must be in colour mode");
@@ -856,8 +927,12 @@ int tslb_closure_dataset_add_fine(tslb_closure* c, tslb_ctx* fine, float pi_scal
     CL_TRY(c, cudaStreamSynchronize(fine->stream));
     const int cx = fine->nx / 2, cy = fine->ny / 2, cz = fine->nz / 2;
     const long long nc = (long long)cx * cy * cz;
+    if (z_hi <= 0 || z_hi > cz) z_hi = cz;
+    if (z_lo < 0 || z_lo >= z_hi) return cfail(c, TSLB_ERR_ARG, "tslb_closure_dataset_add_fine: empty z range");
     const int phase = c->fine_adds % keep_every;
-    const long long nadd = nc > phase ? (nc - phase + keep_every - 1) / keep_every : 0;
+    const long long plane = (long long)cx * cy;
+    const long long J0 = z_lo * plane + phase, J1 = z_hi * plane;
+    const long long nadd = J1 > J0 ? (J1 - J0 + keep_every - 1) / keep_every : 0;
     int rc = grow_dataset(c, c->ds_n + nadd);
     if (rc) return rc;
     float* inter = nullptr;
@@ -867,7 +942,7 @@ int tslb_closure_dataset_add_fine(tslb_closure* c, tslb_ctx* fine, float pi_scal
     if (e == cudaSuccess && nadd > 0) {
         samples_kernel<<<(unsigned)((nadd + 255) / 256), 256, 0, c->stream>>>(
             inter, cx, cy, cz, fine->p.bc[0] == TSLB_BC_PERIODIC, fine->p.bc[2] == TSLB_BC_PERIODIC,
-            fine->p.bc[4] == TSLB_BC_PERIODIC, keep_every, phase, c->ds_n, c->ds_feat, c->ds_tgt, c->ds_wgt);
+            fine->p.bc[4] == TSLB_BC_PERIODIC, keep_every, J0, J1, c->ds_n, c->ds_feat, c->ds_tgt, c->ds_wgt);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -949,12 +1024,14 @@ int tslb_closure_features(tslb_closure* c, tslb_ctx* L, float* features) {
     if (L->p.mode != TSLB_MODE_COLOUR || L->p.precision != TSLB_PREC_FP32)
         return cfail(c, TSLB_ERR_ARG, "tslb_closure_features: colour mode with FP32 storage only");
     if (!L->loaded) return cfail(c, TSLB_ERR_STATE, "the lattice has no state");
-    if (tslb_internal::ensure_dtau(L)) return cfail(c, TSLB_ERR_CUDA, L->err);
     const float* view = nullptr;
     if (tslb_internal::fp32_view(L, &view)) return cfail(c, TSLB_ERR_CUDA, L->err);
     float* d = nullptr;
     CL_TRY(c, cudaMalloc(&d, sizeof(float) * NFEAT * L->n));
-    features_kernel<<<(unsigned)((L->n + 255) / 256), 256, 0, L->stream>>>(lattice_src(L, view), d);
+    // the correction in effect: the closure's total, the static field, or none
+    LatticeSrc src = lattice_src(L, view);
+    src.dtau = L->closure ? L->dtau : (L->base_on ? L->dtau_base : nullptr);
+    features_kernel<<<(unsigned)((L->n + 255) / 256), 256, 0, L->stream>>>(src, d);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(features, d, sizeof(float) * NFEAT * L->n, cudaMemcpyDeviceToHost, L->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
@@ -967,7 +1044,6 @@ int tslb_attach_closure(tslb_ctx* L, tslb_closure* c, int interval) {
     if (!L) return TSLB_ERR_ARG;
     if (!c) {
         L->closure = nullptr;
-        L->dtau_on = false;
         return TSLB_OK;
     }
     if (interval < 1) return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: interval must be >= 1");
@@ -976,11 +1052,17 @@ int tslb_attach_closure(tslb_ctx* L, tslb_closure* c, int interval) {
     if (c->device != L->device) return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: closure and lattice on different devices");
     int rc = tslb_internal::ensure_dtau(L);
     if (rc) return rc;
+    // the first refresh sees the static correction as the previous total
+    if (L->base_on) {
+        if (cudaMemcpyAsync(L->dtau, L->dtau_base, sizeof(float) * L->n, cudaMemcpyDeviceToDevice, L->stream) != cudaSuccess)
+            return tslb_internal::fail(L, TSLB_ERR_CUDA, "tslb_attach_closure: copy of the static correction");
+    } else if (cudaMemsetAsync(L->dtau, 0, sizeof(float) * L->N, L->stream) != cudaSuccess) {
+        return tslb_internal::fail(L, TSLB_ERR_CUDA, "tslb_attach_closure: clearing the correction");
+    }
     // the closure's own queued work (parameter uploads, training) precedes the lattice's use of it
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return tslb_internal::fail(L, TSLB_ERR_CUDA, "closure stream");
     L->closure = c;
     L->closure_interval = interval;
-    L->dtau_on = true;
     return TSLB_OK;
 }
 

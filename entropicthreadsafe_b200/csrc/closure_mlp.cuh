@@ -31,16 +31,26 @@ constexpr int P_W1 = 0, P_B1 = 1024, P_W2 = 1088, P_B2 = 5184, P_W3 = 5248, P_B3
 constexpr int NPARAM_PAD = 5320;
 constexpr int PSTRIDE = NPARAM_PAD + 8;  // per-CTA partial gradient; loss sum at NPARAM_PAD
 
-// TMEM columns
+// TMEM columns of the training kernel (inference uses column 0 for both layers)
 constexpr uint32_t COL_Z1 = 0, COL_Z2 = 64, COL_DH1 = 0, COL_DW = 128;
 
-constexpr int ACT_GROUP = 12 * 128, DZ_GROUP = 16 * 128;   // bytes per row group
-constexpr int ACT_BYTES = 16 * ACT_GROUP, DZ_BYTES = 16 * DZ_GROUP;
+// ACT holds NCH 16-byte chunks per row: 12 in training (h1 | x | 1 | 0),
+// 10 in inference (h1 | x)
+constexpr int NCH_TRAIN = 12, NCH_INFER = 10;
+template <int NCH>
+struct Act {
+    static constexpr int GROUP = NCH * 128;   // bytes per row group of 8 rows
+    static constexpr int BYTES = 16 * GROUP;
+    __device__ static __forceinline__ int chunk(int s, int c) { return (s >> 3) * (NCH * 8) + c * 8 + (s & 7); }
+};
+constexpr int ACT_GROUP = Act<NCH_TRAIN>::GROUP, DZ_GROUP = 16 * 128;   // bytes per row group
+constexpr int ACT_BYTES = Act<NCH_TRAIN>::BYTES, DZ_BYTES = 16 * DZ_GROUP;
 
 // The network in the form the kernels read it (device memory; copied into
 // shared memory at kernel start).
 struct __align__(128) Image {
-    uint4 w1[128];   // W1, K-major B: 16-byte chunk (unit n, k-chunk kc) at (n/8)*16 + kc*8 + n%8
+    uint4 w1[128];   // W1, K-major B: 16-byte chunk (unit n, k-chunk kc) at (n/8)*16 + kc*8 + n%8;
+                     // column 10 holds b1 (input 10 is a constant 1)
     uint4 w2[512];   // W2, K-major B: chunk (n, kc) at (n/8)*64 + kc*8 + n%8
     float b1[NH], b2[NH], w3[NH];   // w3 holds BF16-rounded values
     float b3, dtau_max, pad0[2];
@@ -50,7 +60,7 @@ constexpr int IMG_BYTES = (int)((sizeof(Image) + 127) / 128 * 128);
 
 __host__ __device__ constexpr int w1_chunk(int n, int kc) { return (n >> 3) * 16 + kc * 8 + (n & 7); }
 __host__ __device__ constexpr int w2_chunk(int n, int kc) { return (n >> 3) * 64 + kc * 8 + (n & 7); }
-__device__ __forceinline__ int act_chunk(int s, int c) { return (s >> 3) * 96 + c * 8 + (s & 7); }
+__device__ __forceinline__ int act_chunk(int s, int c) { return Act<NCH_TRAIN>::chunk(s, c); }
 __device__ __forceinline__ int dz_chunk(int s, int c) { return (s >> 3) * 128 + c * 8 + (s & 7); }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -62,14 +72,16 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
 }
 
 // ---- MMA issue (one thread) ----
-__device__ __forceinline__ void issue_fwd1(uint32_t tb, uint32_t act, uint32_t w1) {
-    tc::mma_bf16(tb + COL_Z1, tc::sdesc(act + 8 * 128, 128, ACT_GROUP), tc::sdesc(w1, 128, 256),
+template <int NCH = NCH_TRAIN>
+__device__ __forceinline__ void issue_fwd1(uint32_t tb, uint32_t act, uint32_t w1, uint32_t col = COL_Z1) {
+    tc::mma_bf16(tb + col, tc::sdesc(act + 8 * 128, 128, Act<NCH>::GROUP), tc::sdesc(w1, 128, 256),
                  tc::idesc_bf16(128, 64, 0, 0), 0u);
 }
-__device__ __forceinline__ void issue_fwd2(uint32_t tb, uint32_t act, uint32_t w2) {
+template <int NCH = NCH_TRAIN>
+__device__ __forceinline__ void issue_fwd2(uint32_t tb, uint32_t act, uint32_t w2, uint32_t col = COL_Z2) {
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk)
-        tc::mma_bf16(tb + COL_Z2, tc::sdesc(act + kk * 256, 128, ACT_GROUP), tc::sdesc(w2 + kk * 256, 128, 1024),
+        tc::mma_bf16(tb + col, tc::sdesc(act + kk * 256, 128, Act<NCH>::GROUP), tc::sdesc(w2 + kk * 256, 128, 1024),
                      tc::idesc_bf16(128, 64, 0, 0), kk > 0 ? 1u : 0u);
 }
 // dL/dh1 = dz2 W2: A = dz2 (K-major, k = output unit), B = W2 read MN-major
@@ -114,13 +126,16 @@ __device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& ph, int* abort
     return ok;
 }
 
-// normalised input row -> ACT chunks 8, 9
+// normalised input row -> ACT chunks 8, 9; input 10 is a constant 1 that
+// carries the first layer's bias (stored in W1's column 10)
+template <int NCH = NCH_TRAIN>
 __device__ __forceinline__ void put_x(uint4* act, int s, const float* f, const Image& im, bool valid) {
     float x[KIN];
 #pragma unroll
     for (int k = 0; k < KIN; ++k) x[k] = (valid && k < NFEAT) ? (f[k] - im.mu[k]) * im.isd[k] : 0.f;
-    act[act_chunk(s, 8)] = pack8(x);
-    act[act_chunk(s, 9)] = pack8(x + 8);
+    x[NFEAT] = valid ? 1.f : 0.f;
+    act[Act<NCH>::chunk(s, 8)] = pack8(x);
+    act[Act<NCH>::chunk(s, 9)] = pack8(x + 8);
 }
 
 __device__ __forceinline__ uint32_t lane_addr(uint32_t tb, uint32_t col) {
@@ -128,72 +143,71 @@ __device__ __forceinline__ uint32_t lane_addr(uint32_t tb, uint32_t col) {
     return tb + ((32u * warp) << 16) + col;
 }
 
-// z1 -> h1 = relu(z1 + b1) into ACT chunks 0..7; returns the mask z1 + b1 > 0
-__device__ __forceinline__ uint64_t epi_h1(uint32_t tb, uint4* act, int s, const Image& im) {
+// z1 (bias included) -> h1 = relu(z1) into ACT chunks 0..7; MASK: also
+// returns the bits z1 > 0 (training)
+template <int NCH, bool MASK>
+__device__ __forceinline__ uint64_t epi_h1(uint32_t tb, uint4* act, int s, uint32_t col) {
     uint64_t mask = 0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float z[16];
-        tc::tmem_ld16(lane_addr(tb, COL_Z1 + 16 * q), z);
+    for (int q = 0; q < 2; ++q) {
+        float z[32];
+        tc::tmem_ld32(lane_addr(tb, col + 32 * q), z);
+        if (MASK) {
+            uint32_t m = 0;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const float v = z[j] + im.b1[16 * q + j];
-            const bool p = v > 0.f;
-            z[j] = p ? v : 0.f;
-            mask |= (uint64_t)p << (16 * q + j);
+            for (int j = 0; j < 32; ++j) m |= (z[j] > 0.f ? 1u : 0u) << j;
+            mask |= (uint64_t)m << (32 * q);
         }
-        act[act_chunk(s, 2 * q)] = pack8(z);
-        act[act_chunk(s, 2 * q + 1)] = pack8(z + 8);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) z[j] = fmaxf(z[j], 0.f);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) act[Act<NCH>::chunk(s, 4 * q + c)] = pack8(z + 8 * c);
     }
     return mask;
 }
 
-// network output o = w3 . relu(z2 + b2) + b3
-__device__ __forceinline__ float epi_out(uint32_t tb, const Image& im) {
-    float o = im.b3;
+// network output o = w3 . relu(z2 + b2) + b3 (four partial sums)
+__device__ __forceinline__ float epi_out(uint32_t tb, const Image& im, uint32_t col = COL_Z2) {
+    float o[4] = {im.b3, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float z[16];
-        tc::tmem_ld16(lane_addr(tb, COL_Z2 + 16 * q), z);
+    for (int q = 0; q < 2; ++q) {
+        float z[32];
+        tc::tmem_ld32(lane_addr(tb, col + 32 * q), z);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const float v = z[j] + im.b2[16 * q + j];
-            o = fmaf(im.w3[16 * q + j], v > 0.f ? v : 0.f, o);
-        }
+        for (int j = 0; j < 32; ++j) o[j & 3] = fmaf(im.w3[32 * q + j], fmaxf(z[j] + im.b2[32 * q + j], 0.f), o[j & 3]);
     }
-    return o;
+    return (o[0] + o[1]) + (o[2] + o[3]);
 }
 
 // dz2 = g w3 [z2 + b2 > 0] into DZ chunks 0..7; dw3 += g h2
 __device__ __forceinline__ void epi_dz2(uint32_t tb, uint4* dz, int s, const Image& im, float g, float* dw3) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float z[16], d[16];
+    for (int q = 0; q < 2; ++q) {
+        float z[32], d[32];
+        tc::tmem_ld32(lane_addr(tb, COL_Z2 + 32 * q), z);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) d[j] = 0.f;
-        tc::tmem_ld16(lane_addr(tb, COL_Z2 + 16 * q), z);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const float v = z[j] + im.b2[16 * q + j];
+        for (int j = 0; j < 32; ++j) {
+            const float v = z[j] + im.b2[32 * q + j];
             const bool p = v > 0.f;
-            dw3[16 * q + j] = fmaf(g, p ? v : 0.f, dw3[16 * q + j]);
-            d[j] = p ? g * im.w3[16 * q + j] : 0.f;
+            dw3[32 * q + j] = fmaf(g, p ? v : 0.f, dw3[32 * q + j]);
+            d[j] = p ? g * im.w3[32 * q + j] : 0.f;
         }
-        dz[dz_chunk(s, 2 * q)] = pack8(d);
-        dz[dz_chunk(s, 2 * q + 1)] = pack8(d + 8);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dz[dz_chunk(s, 4 * q + c)] = pack8(d + 8 * c);
     }
 }
 
-// dz1 = dh1 [z1 + b1 > 0] into DZ chunks 8..15
+// dz1 = dh1 [z1 > 0] into DZ chunks 8..15
 __device__ __forceinline__ void epi_dz1(uint32_t tb, uint4* dz, int s, uint64_t mask) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float z[16];
-        tc::tmem_ld16(lane_addr(tb, COL_DH1 + 16 * q), z);
+    for (int q = 0; q < 2; ++q) {
+        float z[32];
+        tc::tmem_ld32(lane_addr(tb, COL_DH1 + 32 * q), z);
+        const uint32_t m = (uint32_t)(mask >> (32 * q));
 #pragma unroll
-        for (int j = 0; j < 16; ++j) z[j] = ((mask >> (16 * q + j)) & 1u) ? z[j] : 0.f;
-        dz[dz_chunk(s, 8 + 2 * q)] = pack8(z);
-        dz[dz_chunk(s, 9 + 2 * q)] = pack8(z + 8);
+        for (int j = 0; j < 32; ++j) z[j] = ((m >> j) & 1u) ? z[j] : 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dz[dz_chunk(s, 8 + 4 * q + c)] = pack8(z + 8 * c);
     }
 }
 

@@ -62,7 +62,7 @@ int validate(const tslb_params* p, int nx, int ny, int nz, std::string& why) {
     for (int a = 0; a < 3; ++a)
         if (!std::isfinite(p->force[a])) { why = "non-finite force"; return TSLB_ERR_ARG; }
     for (int f = 0; f < 6; ++f) {
-        if (p->bc[f] < TSLB_BC_PERIODIC || p->bc[f] > TSLB_BC_OUTLET) { why = "unknown boundary kind"; return TSLB_ERR_ARG; }
+        if (p->bc[f] < TSLB_BC_PERIODIC || p->bc[f] > TSLB_BC_PRESSURE) { why = "unknown boundary kind"; return TSLB_ERR_ARG; }
         for (int a = 0; a < 3; ++a)
             if (!std::isfinite(p->bc_u[f][a])) { why = "non-finite wall velocity"; return TSLB_ERR_ARG; }
     }
@@ -95,7 +95,7 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
         a.face[f].plane = c->inlet[f];
     }
     a.flags = c->flags;
-    a.dtau = c->dtau_on ? c->dtau : nullptr;
+    a.dtau = c->closure ? c->dtau : (c->base_on ? c->dtau_base : nullptr);
     for (int f = 0; f < NF; ++f) {
         a.scale[f] = c->scale[f];
         a.iscale[f] = 1.0f / c->scale[f];
@@ -248,6 +248,32 @@ __global__ void reduce_kernel(const float* __restrict__ s, long long n, long lon
         for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) m = fmaxf(m, shmax[w8]);
         atomicMax(reinterpret_cast<unsigned int*>(&red[RED_SLOTS]), __float_as_uint(m));
     }
+}
+
+// splitmix64 finaliser (Steele, Lea, Flood 2014)
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Jet inlet plane: inside the disc normal velocity speed (1 + amp xi) and
+// phi = +1, outside zero velocity and phi = -1; xi in [-1, 1) from a hash of
+// (seed, counter, plane index).  n0 is the first in-plane extent; `axis` and
+// `sign` give the normal component and its direction into the lattice.
+__global__ void inlet_disc_kernel(float* plane, int n0, int n1, int axis, float sign, float c0, float c1, float r2,
+                                  float speed, float amp, unsigned long long seed, unsigned long long counter) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long pa = (long long)n0 * n1;
+    if (i >= pa) return;
+    const float d0 = (float)(i % n0) - c0, d1 = (float)(i / n0) - c1;
+    const bool in = __fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)) <= r2;
+    const unsigned long long h = mix64(mix64(seed * 0x9E3779B97F4A7C15ull + counter) ^ (unsigned long long)i);
+    const float xi = __fsub_rn(__fmul_rn((float)(h >> 40), 1.0f / 8388608.0f), 1.0f);
+    const float wn = in ? __fmul_rn(sign * speed, __fadd_rn(1.0f, __fmul_rn(amp, xi))) : 0.0f;
+    for (int k = 0; k < 3; ++k) plane[k * pa + i] = k == axis ? wn : 0.0f;
+    plane[3 * pa + i] = in ? 1.0f : -1.0f;
 }
 
 // running sums of u, v, w, phi and w^2 (time averages of the jet statistics)
@@ -518,6 +544,7 @@ void tslb_destroy(tslb_ctx* c) {
     cudaFree(c->flags);
     cudaFree(c->red);
     cudaFree(c->dtau);
+    cudaFree(c->dtau_base);
     cudaFree(c->stats);
     for (int f = 0; f < 6; ++f) cudaFree(c->inlet[f]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -677,11 +704,27 @@ int tslb_set_inlet(tslb_ctx* c, int face, const float* uvw_phi) {
     return TSLB_OK;
 }
 
+int tslb_set_inlet_disc(tslb_ctx* c, int face, float c0, float c1, float radius, float speed, float amp,
+                        unsigned long long seed, unsigned long long counter) {
+    if (!c) return TSLB_ERR_ARG;
+    if (face < 0 || face > 5) return fail(c, TSLB_ERR_ARG, "tslb_set_inlet_disc: bad face");
+    if (c->p.bc[face] != TSLB_BC_INLET || !c->inlet[face]) return fail(c, TSLB_ERR_ARG, "tslb_set_inlet_disc: face is not an inlet");
+    if (!std::isfinite(c0) || !std::isfinite(c1) || !std::isfinite(radius) || !std::isfinite(speed) || !std::isfinite(amp))
+        return fail(c, TSLB_ERR_ARG, "tslb_set_inlet_disc: non-finite argument");
+    const int ax = face / 2;
+    const int n0 = ax == 0 ? c->ny : c->nx, n1 = ax == 2 ? c->ny : c->nz;
+    const long long pa = (long long)n0 * n1;
+    inlet_disc_kernel<<<(unsigned)((pa + 255) / 256), 256, 0, c->stream>>>(c->inlet[face], n0, n1, ax, (face & 1) ? -1.f : 1.f, c0, c1,
+                                                                          radius * radius, speed, amp, seed, counter);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
 int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
     if (!c) return TSLB_ERR_ARG;
-    if (c->closure) return fail(c, TSLB_ERR_STATE, "tslb_set_tau_correction: a closure is attached");
     if (!dtau) {
-        c->dtau_on = false;
+        c->base_on = false;
         return TSLB_OK;
     }
     if (c->p.mode != TSLB_MODE_COLOUR || c->p.precision != TSLB_PREC_FP32)
@@ -690,21 +733,21 @@ int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
     for (long long i = 0; i < c->n; ++i)
         if (!std::isfinite(dtau[i]) || !(dtau[i] > lo))
             return fail(c, TSLB_ERR_ARG, "tslb_set_tau_correction: non-finite value or tau + dtau <= 1/2");
-    int rc = tslb_internal::ensure_dtau(c);
-    if (rc) return rc;
-    CUDA_TRY(c, cudaMemcpyAsync(c->dtau, dtau, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+    if (!c->dtau_base) CUDA_TRY(c, cudaMalloc(&c->dtau_base, sizeof(float) * c->N));
+    CUDA_TRY(c, cudaMemcpyAsync(c->dtau_base, dtau, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    c->dtau_on = true;
+    c->base_on = true;
     return TSLB_OK;
 }
 
 int tslb_download_tau_correction(tslb_ctx* c, float* dtau) {
     if (!c || !dtau) return fail(c, TSLB_ERR_ARG, "tslb_download_tau_correction: NULL");
-    if (!c->dtau) {
+    const float* src = c->closure ? c->dtau : (c->base_on ? c->dtau_base : nullptr);
+    if (!src) {
         for (long long i = 0; i < c->n; ++i) dtau[i] = 0.f;
         return TSLB_OK;
     }
-    CUDA_TRY(c, cudaMemcpyAsync(dtau, c->dtau, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(dtau, src, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return TSLB_OK;
 }

@@ -30,10 +30,13 @@ struct tslb_ctx {
     bool loaded = false;
     int zchunk = 32;
     long long launches = 0;
-    // per-node tau correction (colour mode, FP32 storage): read by the step
-    // kernel when dtau_on; written by tslb_set_tau_correction or the closure
+    // per-node tau correction (colour mode, FP32 storage): dtau_base is the
+    // static field of tslb_set_tau_correction (e.g. a sponge layer); with a
+    // closure attached the closure writes dtau = dtau_base + its output and
+    // the step reads dtau, otherwise the step reads dtau_base
     float* dtau = nullptr;
-    bool dtau_on = false;
+    float* dtau_base = nullptr;
+    bool base_on = false;
     tslb_closure* closure = nullptr;       // attached closure (not owned)
     int closure_interval = 1;
     long long steps_done = 0;

@@ -176,7 +176,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                 solid = true;
                 const int k = a.face[f].kind;
                 // a later velocity face wins, as the oracle's face loop overwrites in face order
-                if (k == TSLB_BC_VELOCITY || k == TSLB_BC_INLET || k == TSLB_BC_OUTLET) vface = f;
+                if (k == TSLB_BC_VELOCITY || k == TSLB_BC_INLET || k == TSLB_BC_OUTLET || k == TSLB_BC_PRESSURE) vface = f;
             }
         }
         if (!solid) continue;
@@ -219,7 +219,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                 Ub[1] = __ldg(fb.plane + pa + pi);
                 Ub[2] = __ldg(fb.plane + 2 * pa + pi);
                 phib = __ldg(fb.plane + 3 * pa + pi);
-            } else if (fb.kind == TSLB_BC_OUTLET) {
+            } else if (fb.kind == TSLB_BC_OUTLET || fb.kind == TSLB_BC_PRESSURE) {
                 phib = m[F_PHI];
             }
             float Uf[3] = {Ub[0], Ub[1], Ub[2]};  // velocity of the f equilibrium
@@ -228,8 +228,11 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                 if (ax == 0) Uf[0] = m[F_U];
                 else if (ax == 1) Uf[1] = m[F_V];
                 else Uf[2] = m[F_W];
+            } else if (fb.kind == TSLB_BC_PRESSURE) {
+                // pressure outlet: the fluid node's velocity at density 1
+                Uf[0] = m[F_U]; Uf[1] = m[F_V]; Uf[2] = m[F_W];
             }
-            const float d = m[F_D], rho = 1.f + d;
+            const float d = fb.kind == TSLB_BC_PRESSURE ? 0.f : m[F_D], rho = 1.f + d;
             float omega;
             if (MODE == TSLB_MODE_COLOUR) {
                 const float ca = 0.5f * (1.f + m[F_PHI]), cb = 0.5f * (1.f - m[F_PHI]);

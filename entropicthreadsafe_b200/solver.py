@@ -82,6 +82,11 @@ class Lattice:
         planes = np.ascontiguousarray(planes, np.float32)
         self._check(self.L.tslb_set_inlet(self.h, face, capi.fptr(planes)))
 
+    def set_inlet_disc(self, face: int, c0: float, c1: float, radius: float, speed: float, amp: float,
+                       seed: int, counter: int) -> None:
+        """Jet inlet drawn on the device (see tslb_set_inlet_disc; workloads.inlet_disc is its host mirror)."""
+        self._check(self.L.tslb_set_inlet_disc(self.h, face, c0, c1, radius, speed, amp, int(seed), int(counter)))
+
     def set_tau_correction(self, dtau) -> None:
         """Per-node relaxation-time correction (nz, ny, nx), or None to switch it off."""
         if dtau is None:

@@ -7,6 +7,9 @@ workload is the same on every machine and for every rank.
   droplet  64^3 fully periodic static droplet, colour gradient
   channel  384x192x128 two-component channel: x, y periodic, bounce-back
            walls at z, body force gx, 40 droplets of radius 8
+  jet      two-component round jet: 192x192x384 (coarse) or 384x384x768
+           (fine, factor 2 in space and time), disc inlet at z = 0,
+           zero-gradient outlet, x, y periodic
 """
 from __future__ import annotations
 
@@ -122,3 +125,79 @@ def channel(nx: int | None = None, ny: int | None = None, nz: int | None = None,
                 phi[np.ix_(zs, ys, xs)] = np.maximum(sub, blob)
     f["phi"][:] = phi.astype(np.float32)
     return p, f
+
+
+# ---- round jet (the learned-closure workload) ----
+JET = dict(nx=192, ny=192, nz=384, diameter=16.0, w_in=0.08, noise=0.03, nu=8e-4, sigma=0.002, beta=0.7,
+           refresh=10)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser on uint64 arrays (wrapping arithmetic)."""
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def inlet_disc(n0: int, n1: int, axis: int, sign: float, c0: float, c1: float, radius: float, speed: float,
+               amp: float, seed: int, counter: int) -> np.ndarray:
+    """Host mirror of tslb_set_inlet_disc: the (4, n1, n0) plane (u, v, w, phi)."""
+    i = np.arange(n0 * n1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        k = np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15) + np.uint64(counter)
+    h = _mix64(_mix64(np.array([k], np.uint64))[0] ^ i)
+    xi = (h >> np.uint64(40)).astype(np.float32) * np.float32(1.0 / 8388608.0) - np.float32(1.0)
+    d0 = (np.arange(n0 * n1) % n0).astype(np.float32) - np.float32(c0)
+    d1 = (np.arange(n0 * n1) // n0).astype(np.float32) - np.float32(c1)
+    inside = d0 * d0 + d1 * d1 <= np.float32(radius) * np.float32(radius)
+    wn = (np.float32(sign) * np.float32(speed)) * (np.float32(1.0) + np.float32(amp) * xi)
+    out = np.zeros((4, n0 * n1), np.float32)
+    out[axis] = np.where(inside, wn, np.float32(0.0))
+    out[3] = np.where(inside, np.float32(1.0), np.float32(-1.0))
+    return out.reshape(4, n1, n0)
+
+
+def jet(scale: int = 1, **over):
+    """Round jet of component A (phi = +1) into quiescent B (phi = -1).
+
+    scale 1: 192 x 192 x 384, disc diameter 16, nu 8e-4, sigma 0.002.
+    scale 2: 384 x 384 x 768 at the same Reynolds and Weber numbers under
+    acoustic scaling (dx and dt halved, lattice velocities unchanged):
+    diameter 32, nu and sigma doubled, and the inlet noise refreshed every
+    2 x 10 steps.  x, y periodic; inlet face z- (TSLB_BC_INLET, drawn by
+    jet_inlet); outlet z+ with zero-gradient velocity and phi at density 1
+    (TSLB_BC_PRESSURE: the reference's zero-gradient outlet, which also
+    copies the density, grows without bound at this viscosity).  Returns
+    (params, fields, spec)."""
+    cfg = dict(JET)
+    cfg.update(over)
+    nx, ny, nz = scale * cfg["nx"], scale * cfg["ny"], scale * cfg["nz"]
+    nu = cfg["nu"] * scale
+    tau = 3.0 * nu + 0.5
+    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=cfg["sigma"] * scale, beta=cfg["beta"],
+                         grad_threshold=1e-3, bc=[capi.BC_PERIODIC] * 4 + [capi.BC_INLET, capi.BC_PRESSURE],
+                         bc_phi=[-1.0] * 6, wall_phi_mode=1)
+    f = empty_fields(nx, ny, nz)
+    f["phi"][:] = -1.0
+    spec = dict(nx=nx, ny=ny, nz=nz, scale=scale, diameter=cfg["diameter"] * scale, w_in=cfg["w_in"],
+                noise=cfg["noise"], refresh=cfg["refresh"] * scale, cx=nx / 2 - 0.5, cy=ny / 2 - 0.5, tau=tau)
+    return p, f, spec
+
+
+def jet_sponge(spec: dict, frac: float = 0.15, amp: float = 0.3) -> np.ndarray:
+    """Sponge layer in front of the outlet: a static tau correction rising as
+    amp * scale * s^2 over the last `frac` of the length (s from 0 to 1), so
+    eddies are damped before the outlet.  (nz, ny, nx) float32."""
+    nz, ny, nx = spec["nz"], spec["ny"], spec["nx"]
+    z0 = (1.0 - frac) * nz
+    z = np.arange(nz) + 0.5
+    prof = np.where(z > z0, ((z - z0) / (nz - z0)) ** 2, 0.0) * amp * spec["scale"]
+    return np.broadcast_to(prof.astype(np.float32)[:, None, None], (nz, ny, nx))
+
+
+def jet_inlet(lat, spec: dict, seed: int, step: int) -> None:
+    """Draw the jet inlet of `step` on the device (refreshed every spec['refresh'] steps)."""
+    lat.set_inlet_disc(4, spec["cx"], spec["cy"], spec["diameter"] / 2, spec["w_in"], spec["noise"], seed,
+                       step // spec["refresh"])

@@ -79,6 +79,13 @@ extern "C" {
 #define TSLB_BC_INLET         3  /* regularized inlet, per-node velocity and colour plane
                                     (bcs_2c_turbulent_jet inlet, :931-988)                */
 #define TSLB_BC_OUTLET        4  /* regularized zero-gradient outlet (:990-1048)          */
+#define TSLB_BC_PRESSURE      5  /* regularized pressure outlet: density 1, velocity and
+                                    phi of the fluid node (zero gradient).  No reference
+                                    counterpart: the reference outlet (kind 4) takes the
+                                    density of the fluid node too, which lets density and
+                                    velocity drift together at low viscosity (in a jet at
+                                    tau 0.5024 the outlet planes grow without bound within
+                                    ~2700 steps); fixing the density removes that mode.   */
 
 #define TSLB_NREDUCE         12
 
@@ -164,16 +171,31 @@ int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
  * four planes (u, v, w, phi) of the face's extent, Fortran order. */
 int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
 
-/* Per-node correction dtau of the relaxation time (colour mode, FP32
- * storage): node x relaxes with tau(phi_x) + dtau[x], i.e. an added local
- * viscosity dtau/3, in the collision and in the regularized faces; the
+/* Jet inlet drawn on the device (asynchronous, no host copy): the plane of
+ * inlet face `face` becomes a disc of radius `radius` centred at in-plane
+ * coordinates (c0, c1) -- (x, y) for z faces, (x, z) for y faces, (y, z)
+ * for x faces, node indices from 0 -- with normal velocity
+ * speed * (1 + amp * xi) into the lattice and phi = +1; outside the disc the
+ * velocity is 0 and phi = -1.  xi is uniform in [-1, 1): the top 24 bits of
+ * h = m(m(seed * 0x9E3779B97F4A7C15 + counter) ^ i), m the splitmix64
+ * finaliser and i the plane index (first coordinate fastest), times 2^-23,
+ * minus 1.  Replaces the host random_number refresh of the jet inlet
+ * (boundary_cds_3D_module.f90:866-877); call it with counter = step / 10
+ * to refresh every 10 steps. */
+int  tslb_set_inlet_disc(tslb_ctx* ctx, int face, float c0, float c1, float radius, float speed, float amp,
+                         unsigned long long seed, unsigned long long counter);
+
+/* Static per-node correction dtau of the relaxation time (colour mode,
+ * FP32 storage): node x relaxes with tau(phi_x) + dtau[x], i.e. an added
+ * local viscosity dtau/3, in the collision and in the regularized faces; the
  * surface-tension coefficient follows the corrected omega.  dtau holds
  * nx*ny*nz values (Fortran order) with tau + dtau > 1/2; NULL switches the
- * correction off.  The reference has no counterpart: it is the hook of the
- * learned eddy-viscosity closure (tslb_closure.h), which writes the same
- * buffer on the device. */
+ * correction off.  Typical use: a sponge layer in front of an outlet.  With
+ * a learned closure attached (tslb_closure.h) the closure's output is added
+ * to this field.  The reference has no counterpart. */
 int  tslb_set_tau_correction(tslb_ctx* ctx, const float* dtau);
-/* The current correction (zeros when none was set). */
+/* The correction in effect (static field plus closure output; zeros when
+ * there is none). */
 int  tslb_download_tau_correction(tslb_ctx* ctx, float* dtau);
 
 /* Time averages on the device: tslb_stats_accumulate adds u, v, w, phi and

@@ -87,12 +87,14 @@ int  tslb_closure_dataset_clear(tslb_closure* c);
 int  tslb_closure_dataset_add(tslb_closure* c, const float* features, const float* target, const float* weight,
                               long long n);
 /* Samples of a fine colour-mode lattice (FP32 storage, even sizes) filtered
- * onto the grid of half its size: every keep_every-th coarse node; Pi^neq is
- * multiplied by pi_scale to express it at the coarse grid's plain tau
- * (2 tau_coarse / tau_fine for acoustic scaling).  *added (may be NULL)
- * receives the number of samples appended. */
+ * onto the grid of half its size: every keep_every-th coarse node of the
+ * coarse planes z_lo <= z < z_hi (z_hi <= 0: to the last plane), starting
+ * at an offset that cycles with each call; Pi^neq is multiplied by pi_scale
+ * to express it at the coarse grid's plain tau (2 tau_coarse / tau_fine for
+ * acoustic scaling).  *added (may be NULL) receives the number of samples
+ * appended. */
 int  tslb_closure_dataset_add_fine(tslb_closure* c, tslb_ctx* fine, float pi_scale, int keep_every,
-                                   long long* added);
+                                   int z_lo, int z_hi, long long* added);
 long long tslb_closure_dataset_size(tslb_closure* c);
 int  tslb_closure_dataset_download(tslb_closure* c, float* features, float* target, float* weight);
 /* mu, sd of the features over the training set; weights rescaled to mean 1. */
@@ -109,9 +111,11 @@ int  tslb_closure_train(tslb_closure* c, int steps, int batch, float lr, unsigne
 int  tslb_closure_features(tslb_closure* c, tslb_ctx* lattice, float* features);
 
 /* Attach (c != NULL) or detach (c == NULL) the closure: before every
- * `interval`-th step the lattice refreshes its per-node tau correction
- * (see tslb_set_tau_correction) from the closure on its own stream.  The
- * closure must outlive the attachment. */
+ * `interval`-th step the lattice refreshes its per-node tau correction from
+ * the closure on its own stream: dtau = static field (tslb_set_tau_correction,
+ * if set) + the network's output; the features' s uses the previous total.
+ * The closure must outlive the attachment; do not train or change an
+ * attached closure while the lattice's stream has work queued. */
 int  tslb_attach_closure(tslb_ctx* lattice, tslb_closure* c, int interval);
 
 const char* tslb_closure_last_error(tslb_closure* c);

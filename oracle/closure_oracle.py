@@ -11,8 +11,9 @@ can check the CUDA kernels:
 - the network's forward pass and the gradient of the weighted squared loss.
 
 `emulate=True` rounds exactly where the tensor-core kernels round to BF16
-(the weights W1, W2, w3, the normalised input, the hidden activation h1 and
-the back-propagated dz2, dz1); everything else is FP64.  `emulate=False` is
+(the weights W1, W2, w3, the first bias b1, which the kernels carry as a
+weight column against a constant input 1, the normalised input, the hidden
+activation h1 and the back-propagated dz2, dz1); everything else is FP64.  `emulate=False` is
 the exact FP64 network (used for finite-difference checks of the backward
 pass).  Only tests/ import this module.
 """
@@ -74,11 +75,11 @@ def normalised_input(F, mu, sd, emulate: bool) -> np.ndarray:
 def forward(p, mu, sd, dtau_max, F, emulate: bool = True):
     """dtau = dtau_max sigmoid(o) for feature rows F; returns (y, cache)."""
     w = unpack(p)
-    W1, W2, w3 = w["W1"], w["W2"], w["w3"]
+    W1, W2, w3, b1 = w["W1"], w["W2"], w["w3"], w["b1"]
     if emulate:
-        W1, W2, w3 = bf16(W1), bf16(W2), bf16(w3)
+        W1, W2, w3, b1 = bf16(W1), bf16(W2), bf16(w3), bf16(b1)
     x = normalised_input(F, mu, sd, emulate)
-    z1 = x @ W1.T + w["b1"]
+    z1 = x @ W1.T + b1
     m1 = z1 > 0
     h1 = np.where(m1, z1, 0.0)
     if emulate:

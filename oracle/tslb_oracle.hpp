@@ -164,7 +164,7 @@ struct Oracle {
     int dim(int a) const { return a == 0 ? nx : a == 1 ? ny : nz; }
     bool periodic(int a) const { return prm.bc[2 * a] == TSLB_BC_PERIODIC; }
     static bool velocity_kind(int bc) {
-        return bc == TSLB_BC_VELOCITY || bc == TSLB_BC_INLET || bc == TSLB_BC_OUTLET;
+        return bc == TSLB_BC_VELOCITY || bc == TSLB_BC_INLET || bc == TSLB_BC_OUTLET || bc == TSLB_BC_PRESSURE;
     }
     R& F(int q, int i, int j, int k) { return f[size_t(q) * vol + id(i, j, k)]; }
     R& G(int q, int i, int j, int k) { return g[size_t(q) * vol + id(i, j, k)]; }
@@ -467,6 +467,13 @@ struct Oracle {
             Ub[axis] = uvw[axis];
             phib = phi;
         }
+        R rho_b = rho;
+        if (bc == TSLB_BC_PRESSURE) {
+            // pressure outlet (no reference counterpart): density 1, the node's velocity and phi
+            for (int a = 0; a < 3; ++a) Ub[a] = uvw[a];
+            phib = phi;
+            rho_b = R(1);
+        }
         R omega;
         if (colour) {
             const R nu_a = (R(prm.tau_a) - R(0.5)) / R(3), nu_b = (R(prm.tau_b) - R(0.5)) / R(3);
@@ -477,7 +484,7 @@ struct Oracle {
             omega = omega_pf();
         }
         const R wq = W.w(q);
-        R val = wq * feq_over_w<R>(q, rho, Ub[0], Ub[1], Ub[2]) + (R(1) - omega) * wq * aneq<R>(q, P, u, v, w);
+        R val = wq * feq_over_w<R>(q, rho_b, Ub[0], Ub[1], Ub[2]) + (R(1) - omega) * wq * aneq<R>(q, P, u, v, w);
         if (colour) {
             F(q, i, j, k) = val * (R(1) + phib) / R(2);
             G(q, i, j, k) = val * (R(1) - phib) / R(2);
@@ -497,7 +504,7 @@ struct Oracle {
         if (bc == TSLB_BC_INLET) {
             for (int a = 0; a < 3; ++a) Ub[a] = inlet_val(fc, a, i, j, k);
             phib = inlet_val(fc, 3, i, j, k);
-        } else if (bc == TSLB_BC_OUTLET) {
+        } else if (bc == TSLB_BC_OUTLET || bc == TSLB_BC_PRESSURE) {
             phib = phi;
         }
         const R eu = R(GX[q]) * Ub[0] + R(GY[q]) * Ub[1] + R(GZ[q]) * Ub[2];

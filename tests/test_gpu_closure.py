@@ -145,11 +145,12 @@ def test_dataset_from_fine_lattice_matches_oracle():
     with Lattice(p, nx, ny, nz) as lat, Closure() as c:
         lat.upload_moments(f)
         n0 = c.dataset_add_fine(lat, 1.9, keep_every=3)
-        n1 = c.dataset_add_fine(lat, 1.9, keep_every=3)
+        n1 = c.dataset_add_fine(lat, 1.9, keep_every=3, z_range=(2, 13))
         feat, tgt, wgt = c.dataset()
     rf, rt, rw = co.fine_samples({k: v.astype(np.float32) for k, v in f.items()}, 1.9, (True, True, False))
     nc = rf.shape[0]
-    sel = np.concatenate([np.arange(0, nc, 3), np.arange(1, nc, 3)])
+    plane = (nx // 2) * (ny // 2)
+    sel = np.concatenate([np.arange(0, nc, 3), np.arange(2 * plane + 1, 13 * plane, 3)])
     assert n0 + n1 == len(sel) == feat.shape[0]
     scale = np.abs(rf).max(axis=0) + 1e-30
     assert (np.abs(feat - rf[sel]) / scale).max() <= 2e-6
@@ -205,9 +206,13 @@ def test_attached_closure_step_matches_oracle():
     mu = feats.mean(0).astype(np.float32)
     sd = (feats.std(0) + 1e-12).astype(np.float32)
     nsteps = 3
+    # a static correction (a sponge on the last planes) under the closure's output
+    base = np.zeros((nz, ny, nx), np.float32)
+    base[-6:] = np.linspace(0.01, 0.1, 6, dtype=np.float32)[:, None, None]
     with Lattice(p, nx, ny, nz) as lat, closure_with(net, mu, sd, dm) as c:
         lat.set_inlet(4, pl)
         lat.upload_moments(f)
+        lat.set_tau_correction(base)
         lattice_attach(lat, c, 1)
         lat.step(nsteps)
         got = lat.download()
@@ -216,18 +221,18 @@ def test_attached_closure_step_matches_oracle():
     o = oracle.Oracle(p, nx, ny, nz, fp64=True)
     o.set_inlet(4, pl.astype(np.float64))
     o.set_moments({k: np.asarray(v, np.float64) for k, v in f.items()})
-    dtp = np.zeros((nz, ny, nx))
+    dtp = base.astype(np.float64)
     for _ in range(nsteps):
         st = o.get_moments()
         y, _ = co.forward(net, mu, sd, dm, co.lattice_features(st, p.tau_a, p.tau_b, (True, True, False), dtp),
                           emulate=True)
-        dtp = y.reshape(nz, ny, nx)
+        dtp = y.reshape(nz, ny, nx) + base
         o.set_tau_correction(dtp)
         o.step(1)
     ref = o.get_moments()
     o.close()
     assert np.abs(dt_gpu - dtp).max() <= 5e-3 * dm
-    assert dtp.std() > 0.02 * dm   # the correction varies in space
+    assert (dtp - base).std() > 0.02 * dm   # the correction varies in space
     errs = field_errors(got, ref)
     assert max(errs.values()) <= 1e-4, errs
 

@@ -96,6 +96,19 @@ def test_phasefield_jet_inlet_outlet():
     assert_parity(gpu, o64, o32, "phase-field jet")
 
 
+def test_colour_jet_inlet_pressure_outlet():
+    """Colour jet: device-drawn disc inlet at z-, pressure outlet at z+."""
+    p, f, spec = workloads.jet(1, nx=20, ny=18, nz=24, diameter=6.0, nu=0.02)
+    planes = workloads.inlet_disc(20, 18, 2, 1.0, spec["cx"], spec["cy"], 3.0, spec["w_in"], spec["noise"], 9, 0)
+    inlet = {capi.FACE_ZM: planes}
+    gpu, _ = run_gpu(p, f, 80, inlet=inlet)
+    o64, _ = run_oracle(p, f, 80, fp64=True, inlet=inlet)
+    o32, _ = run_oracle(p, f, 80, fp64=False, inlet=inlet)
+    assert_parity(gpu, o64, o32, "colour jet, pressure outlet")
+    # the pressure outlet holds the outlet density near 1
+    assert abs(float(np.mean(o64["rho"][-1])) - 1.0) < 2e-3
+
+
 def test_phasefield_droplet_bounceback_all_faces():
     n = 20
     p = capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=0.7, sigma=0.01, sharp_c=0.9,
