@@ -3,17 +3,20 @@ vs fine plain).
 
     python -m entropicthreadsafe_b200.closure_study [--out result.json] [--shrink K]
 
-1. Fine plain runs (384 x 384 x 768, two inlet-noise seeds) feed the
-   training set: snapshots of their state, box-filtered onto the coarse
-   grid (tslb_closure_dataset_add_fine).
+1. Fine plain runs (384 x 384 x 768, three inlet-noise seeds) are the
+   judge: their time-averaged fields, averaged over the seeds, give the
+   reference jet statistics, and the spread over the seeds is the noise
+   floor of one realisation.  Snapshots of two of them, box-filtered onto
+   the coarse grid (tslb_closure_dataset_add_fine), are the training set;
+   snapshots of the third test the network a priori.
 2. The network is trained on the GPU (tslb_closure_train).
-3. A third fine plain run (another seed) is the judge: its time-averaged
-   fields give the reference jet statistics, and snapshots of it give a
-   held-out a-priori test of the network.
-4. Coarse plain and coarse + closure runs (192 x 192 x 384, the judge's
-   seed) are compared with the judge on spreading rate, centreline decay
-   and mixing thickness; GPU time (CUDA events on each lattice's stream)
-   is reported for every run.
+3. Coarse plain and coarse + closure runs (192 x 192 x 384, three seeds)
+   are compared, as seed averages, with the fine average on spreading
+   rate, centreline decay and mixing thickness.  The closure runs are
+   repeated with the network's output scaled by a few global gains (an a
+   posteriori calibration, as LES calibrates a Smagorinsky constant); the
+   best gain on these seeds is then checked on three fresh seeds.  GPU time
+   (CUDA events on each lattice's stream) is reported for every run.
 
 Times are in coarse steps; the fine grid runs twice as many steps
 (acoustic scaling).  --shrink K divides the lattice sizes and the jet
@@ -42,11 +45,12 @@ def _events(stream_handle):
 
 def run_jet(scale: int, seed: int, steps: int, avg_from: int, sample_every: int, over: dict, closure=None,
             interval: int = 1, dataset=None, snaps=(), keep_every: int = 8, pi_scale: float = 2.0,
-            check_every: int = 500, sponge=(0.15, 0.3)) -> dict:
+            check_every: int = 500, sponge=(0.15, 0.3), z_lo: int = 0) -> dict:
     """One jet run; returns its statistics (coarse units), GPU time and state.
 
-    Training samples (dataset) are taken outside the sponge layer, whose
-    added viscosity the fine stresses carry."""
+    Training samples (dataset) are taken from coarse plane z_lo on (past the
+    inlet's top-hat edge) and outside the sponge layer, whose added
+    viscosity the fine stresses carry."""
     p, f, spec = workloads.jet(scale, **over)
     z_hi = int((1.0 - sponge[0]) * spec["nz"] / scale) if sponge is not None else 0
     res = dict(scale=scale, seed=seed, steps=steps, nodes=spec["nx"] * spec["ny"] * spec["nz"],
@@ -72,7 +76,7 @@ def run_jet(scale: int, seed: int, steps: int, avg_from: int, sample_every: int,
                 if done >= avg_from and (done - avg_from) % sample_every == 0:
                     lat.stats_accumulate()
                 if dataset is not None and done in snaps:
-                    res["samples"] += dataset.dataset_add_fine(lat, pi_scale, keep_every, (0, z_hi))
+                    res["samples"] += dataset.dataset_add_fine(lat, pi_scale, keep_every, (z_lo, z_hi))
                     res["snapshots"] += 1
                 if done % check_every == 0:
                     lat.synchronize()
@@ -120,23 +124,61 @@ def _strip(r: dict) -> dict:
     return out
 
 
+def _mean_stats(runs) -> dict | None:
+    """Seed average of the runs' statistics and profiles; 'spread' is the
+    standard deviation over the seeds relative to the mean."""
+    keys = ("spreading_rate", "decay_rate", "mixing_thickness", "centreline_mean")
+    ok = [r["stats"] for r in runs if "stats" in r]
+    if not ok:
+        return None
+    out = {k: float(np.mean([s[k] for s in ok])) for k in keys}
+    out["spread"] = {k: float(np.std([s[k] for s in ok]) / abs(out[k])) if len(ok) > 1 else 0.0 for k in keys}
+    for k in ("wc", "r_half", "delta"):
+        out[k] = np.nanmean(np.stack([np.asarray(s[k], float) for s in ok]), axis=0)
+    out["z"] = ok[0]["z"]
+    out["window"] = ok[0]["window"]
+    return out
+
+
+SCALARS = ("spreading_rate", "decay_rate", "mixing_thickness", "centreline_mean")
+
+
+def _summary(runs, ref) -> dict:
+    ms = _mean_stats(runs)
+    entry = dict(gpu_s=float(np.mean([r["gpu_s"] for r in runs])), diverged=[r["diverged_at"] for r in runs])
+    if ms is not None:
+        entry["mean"] = {k: ms[k] for k in SCALARS}
+        entry["spread"] = ms["spread"]
+        if ref is not None:
+            entry["vs_fine"] = jetstats.compare(ms, ref)
+            entry["score"] = float(np.mean([entry["vs_fine"][k] for k in SCALARS]))
+    return entry
+
+
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--out", default=None)
     ap.add_argument("--shrink", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=16000, help="coarse steps per run")
+    ap.add_argument("--steps", type=int, default=20000, help="coarse steps per run")
     ap.add_argument("--avg-from", type=int, default=8000)
     ap.add_argument("--sample-every", type=int, default=10)
     ap.add_argument("--snap-every", type=int, default=1000)
     ap.add_argument("--keep-every", type=int, default=6)
-    ap.add_argument("--train-seeds", type=int, nargs="*", default=[101, 102])
-    ap.add_argument("--judge-seed", type=int, default=13)
-    ap.add_argument("--train-steps", type=int, default=4000)
-    ap.add_argument("--batch", type=int, default=32768)
+    ap.add_argument("--fine-seeds", type=int, nargs="*", default=[101, 102, 103])
+    ap.add_argument("--train-seeds", type=int, nargs="*", default=[101, 102],
+                    help="fine seeds whose snapshots train the network; the others test it a priori")
+    ap.add_argument("--coarse-seeds", type=int, nargs="*", default=[101, 102, 103],
+                    help="coarse seeds of the comparison and of the gain calibration")
+    ap.add_argument("--check-seeds", type=int, nargs="*", default=[104, 105, 106],
+                    help="fresh coarse seeds that check the calibrated gain")
+    ap.add_argument("--z-lo", type=int, default=4, help="first coarse plane of the training samples")
+    ap.add_argument("--train-steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--dtau-max", type=float, default=0.02)
-    ap.add_argument("--intervals", type=int, nargs="*", default=[1, 2],
-                    help="closure refresh intervals of the coarse + closure runs")
+    ap.add_argument("--interval", type=int, default=2, help="closure refresh interval of the coarse runs")
+    ap.add_argument("--gains", type=float, nargs="*", default=[1.0, 2.0, 4.0, 8.0],
+                    help="output gains of the a posteriori calibration")
     args = ap.parse_args(argv)
     K = args.shrink
     over = {}
@@ -152,14 +194,23 @@ def main(argv=None) -> dict:
 
     closure = Closure()
     closure.set_params(init_params(0), np.zeros(10), np.ones(10), args.dtau_max)
-    # 1. training data from fine plain runs
-    train_runs = []
-    for seed in args.train_seeds:
-        r = run_jet(2, seed, 2 * T, 2 * A, 2 * S, over, dataset=closure, snaps=snaps, keep_every=args.keep_every,
-                    pi_scale=pi_scale)
-        train_runs.append(_strip(r))
-        print(f"fine training run seed {seed}: {r['gpu_s']:.1f} s GPU, {r['samples']} samples", flush=True)
-    result["train_runs"] = train_runs
+    held = Closure()
+    # 1. fine plain runs: training snapshots, held-out snapshots, reference statistics
+    fine_runs = []
+    for seed in args.fine_seeds:
+        train = seed in args.train_seeds
+        r = run_jet(2, seed, 2 * T, 2 * A, 2 * S, over, dataset=closure if train else held,
+                    snaps=snaps if train else snaps[-3:],
+                    keep_every=args.keep_every if train else 4 * args.keep_every, pi_scale=pi_scale,
+                    z_lo=args.z_lo // K)
+        fine_runs.append(r)
+        print(f"fine run seed {seed} ({'training' if train else 'held out'}): {r['gpu_s']:.1f} s GPU, "
+              f"{r['samples']} samples, diverged {r['diverged_at']}", flush=True)
+    ref = _mean_stats(fine_runs)
+    result["fine_runs"] = [_strip(r) for r in fine_runs]
+    result["fine"]["mean"] = {k: ref[k] for k in SCALARS} if ref else None
+    result["fine"]["spread"] = ref["spread"] if ref else None
+    result["fine"]["gpu_s"] = float(np.mean([r["gpu_s"] for r in fine_runs]))
     result["dataset_size"] = closure.dataset_size
     # 2. training
     import torch
@@ -168,36 +219,55 @@ def main(argv=None) -> dict:
     closure.normalize()
     hist = closure.train(args.train_steps, batch=args.batch, lr=args.lr, seed=7)
     train_s = time.perf_counter() - t0
-    result["training"] = dict(gpu_s=train_s, steps=args.train_steps, batch=args.batch,
-                              loss_first=float(hist[:20].mean()), loss_last=float(hist[-20:].mean()),
-                              loss_curve=hist[:: max(1, len(hist) // 50)].round(9).tolist())
-    print(f"training: {train_s:.1f} s, loss {hist[:20].mean():.3e} -> {hist[-20:].mean():.3e}", flush=True)
-    # 3. judge: fine plain with a held-out seed; its snapshots test the network a priori
-    ev = Closure()
-    judge = run_jet(2, args.judge_seed, 2 * T, 2 * A, 2 * S, over, dataset=ev, snaps=snaps[-3:],
-                    keep_every=4 * args.keep_every, pi_scale=pi_scale)
-    F, t, a = ev.dataset()
-    ev.close()
-    result["a_priori"] = a_priori(closure, F, t, a)
-    result["judge"] = _strip(judge)
-    print(f"judge fine run: {judge['gpu_s']:.1f} s GPU; a priori {result['a_priori']}", flush=True)
-    # 4. coarse runs
-    runs = {"coarse_plain": run_jet(1, args.judge_seed, T, A, S, over)}
-    for k in args.intervals:
-        runs[f"coarse_closure_i{k}"] = run_jet(1, args.judge_seed, T, A, S, over, closure=closure, interval=k)
-    for name, r in runs.items():
-        result[name] = _strip(r)
-        if "stats" in judge and "stats" in r:
-            result[name]["vs_fine"] = jetstats.compare(r["stats"], judge["stats"])
-        result[name]["gpu_time_ratio_fine_over_this"] = judge["gpu_s"] / r["gpu_s"]
+    result["training"] = dict(seconds=train_s, steps=args.train_steps, batch=args.batch,
+                              loss_first=float(hist[:50].mean()), loss_last=float(hist[-50:].mean()),
+                              loss_curve=hist[:: max(1, len(hist) // 50)].round(12).tolist())
+    prm = closure.get_params()
+    net = {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in prm.items()}
+    result["network"] = net
+    print(f"training: {train_s:.2f} s, loss {hist[:50].mean():.3e} -> {hist[-50:].mean():.3e}", flush=True)
+    if held.dataset_size:
+        F, t, a = held.dataset()
+        result["a_priori_held_out"] = a_priori(closure, F, t, a)
+        print("a priori (held-out fine seed):", result["a_priori_held_out"], flush=True)
+    held.close()
+    # 3. coarse plain, and coarse + closure at each gain, on the calibration seeds
+    plain = [run_jet(1, sd, T, A, S, over) for sd in args.coarse_seeds]
+    result["coarse_plain"] = _summary(plain, ref)
+    result["coarse_plain"]["runs"] = [_strip(r) for r in plain]
+    print("coarse plain:", result["coarse_plain"].get("vs_fine"), f"{result['coarse_plain']['gpu_s']:.1f} s", flush=True)
+
+    def with_gain(seeds, gain):
+        closure.set_params(np.asarray(net["params"], np.float32), np.asarray(net["mu"], np.float32),
+                           np.asarray(net["sd"], np.float32), net["dtau_max"] * gain)
+        return [run_jet(1, sd, T, A, S, over, closure=closure, interval=args.interval) for sd in seeds]
+
+    result["coarse_closure"] = {}
+    for g in args.gains:
+        rs = with_gain(args.coarse_seeds, g)
+        e = _summary(rs, ref)
+        e["runs"] = [_strip(r) for r in rs]
+        result["coarse_closure"][str(g)] = e
+        print(f"coarse + closure, gain {g}:", e.get("vs_fine"), f"{e['gpu_s']:.1f} s", flush=True)
+    # 4. the best gain on the calibration seeds, checked on fresh seeds
+    scored = {g: e["score"] for g, e in result["coarse_closure"].items() if "score" in e}
+    if scored and args.check_seeds:
+        best = min(scored, key=scored.get)
+        result["best_gain"] = float(best)
+        cp = [run_jet(1, sd, T, A, S, over) for sd in args.check_seeds]
+        cc = with_gain(args.check_seeds, float(best))
+        result["check"] = dict(seeds=args.check_seeds, gain=float(best), plain=_summary(cp, ref),
+                               closure=_summary(cc, ref))
+        print("check seeds: plain", result["check"]["plain"].get("vs_fine"), "\n closure",
+              result["check"]["closure"].get("vs_fine"), flush=True)
+    result["gpu_time_ratio_fine_over_plain"] = result["fine"]["gpu_s"] / result["coarse_plain"]["gpu_s"]
+    result["gpu_time_ratio_fine_over_closure"] = result["fine"]["gpu_s"] / np.mean(
+        [e["gpu_s"] for e in result["coarse_closure"].values()])
+    print("fine mean:", result["fine"]["mean"], "spread", result["fine"]["spread"], flush=True)
     closure.close()
-    print(json.dumps(result["a_priori"], indent=1))
-    for name in runs:
-        print(name, result[name].get("stats"), result[name].get("vs_fine"), f"{result[name]['gpu_s']:.2f} s", flush=True)
-    print("judge", result["judge"].get("stats"), f"{result['judge']['gpu_s']:.2f} s")
     if args.out:
         with open(args.out, "w") as fh:
-            json.dump(result, fh, indent=1)
+            json.dump(result, fh, indent=1, default=float)
     return result
 
 

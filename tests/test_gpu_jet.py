@@ -79,14 +79,19 @@ def test_closure_study_runs_on_a_shrunk_jet(tmp_path):
     from entropicthreadsafe_b200 import closure_study
     out = tmp_path / "study.json"
     r = closure_study.main(["--shrink", "8", "--steps", "4000", "--avg-from", "2000", "--snap-every", "400",
-                            "--keep-every", "2", "--train-steps", "200", "--batch", "4096",
-                            "--train-seeds", "1", "--out", str(out)])
+                            "--keep-every", "2", "--train-steps", "200", "--batch", "4096", "--fine-seeds", "1", "2",
+                            "--train-seeds", "1", "--coarse-seeds", "3", "--check-seeds", "4", "--gains", "1", "2",
+                            "--out", str(out)])
     assert out.exists()
     assert r["dataset_size"] > 1000
     # minibatch losses of a tiny shrunk set are noisy; learning itself is
     # tested in test_gpu_closure (Smagorinsky law)
     assert np.isfinite(r["training"]["loss_last"]) and r["training"]["loss_last"] > 0
-    for name in ("judge", "coarse_plain", "coarse_closure_i1", "coarse_closure_i2"):
-        assert r[name]["diverged_at"] is None, r[name]
-        assert r[name]["gpu_s"] > 0
-    assert np.isfinite(r["a_priori"]["loss_net"])
+    assert np.isfinite(r["a_priori_held_out"]["loss_net"])
+    for run in r["fine_runs"]:
+        assert run["diverged_at"] is None and run["gpu_s"] > 0
+    assert all(d is None for d in r["coarse_plain"]["diverged"])
+    for g in ("1.0", "2.0"):
+        assert all(d is None for d in r["coarse_closure"][g]["diverged"])
+        assert "vs_fine" in r["coarse_closure"][g]
+    assert r["best_gain"] in (1.0, 2.0) and "vs_fine" in r["check"]["closure"]
