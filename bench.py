@@ -266,6 +266,62 @@ def ensemble_leg(args, ndomains: int = 48):
             "speedup_vs_one_at_a_time": ms_seq / ms_graph}
 
 
+def closure_leg(args):
+    """Config 5 cost: the coarse round jet (192 x 192 x 384, sponge, pressure
+    outlet) stepped plain and with the learned closure attached (refresh every
+    step and every 2 steps).  The closure's cost does not depend on its
+    weights, so a seeded initial network stands in for the trained one (the
+    accuracy study is entropicthreadsafe_b200.closure_study)."""
+    import numpy as np
+    import torch
+    from entropicthreadsafe_b200 import workloads
+    from entropicthreadsafe_b200.closure import Closure, init_params, lattice_attach
+    from entropicthreadsafe_b200.solver import Lattice
+    p, f, spec = workloads.jet(1)
+    nodes = spec["nx"] * spec["ny"] * spec["nz"]
+    res = {"workload": "round jet 192x192x384, disc inlet d=16, nu 8e-4", "nodes": nodes, "steps": args.steps}
+    with Lattice(p, spec["nx"], spec["ny"], spec["nz"]) as lat, Closure() as c:
+        c.set_params(init_params(0), np.zeros(10), np.array([1e-4] * 6 + [1.0, 0.3, 0.05, 1e-4]), 0.02)
+        lat.upload_moments(f)
+        lat.set_tau_correction(workloads.jet_sponge(spec))
+        step = [0]
+
+        def advance(k):
+            for _ in range(k):
+                if step[0] % spec["refresh"] == 0:
+                    workloads.jet_inlet(lat, spec, 13, step[0])
+                lat.step(1)
+                step[0] += 1
+
+        advance(300)  # the jet leaves the inlet
+        lat.synchronize()
+        st = torch.cuda.ExternalStream(lat.stream)
+
+        def timed():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            advance(args.warmup)
+            e0.record(st)
+            advance(args.steps)
+            e1.record(st)
+            lat.synchronize()
+            return e0.elapsed_time(e1) / args.steps
+
+        ms = {"plain": timed()}
+        for k in (1, 2):
+            lattice_attach(lat, c, k)
+            ms[f"closure_every_{k}"] = timed()
+        lattice_attach(lat, None)
+    for name, m in ms.items():
+        res[name] = {"value": nodes / (m * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": m}
+    kern = ms["closure_every_1"] - ms["plain"]
+    # inference kernel: reads 10 moment fields + previous and static dtau, writes dtau (52 B/node);
+    # two dense layers 16x64 and 64x64 on the tensor cores (2 * 5120 flop/node)
+    res["closure_kernel"] = {"ms": kern, "bytes_per_node": 52, "tensor_flop_per_node": 10240,
+                             "GB_per_s": 52 * nodes / (kern * 1e-3) / 1e9,
+                             "tensor_TFLOP_per_s": 10240 * nodes / (kern * 1e-3) / 1e12}
+    return res
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -347,6 +403,7 @@ def run_ours(args):
     if lat is not None:
         lat.close()
     ens = None if args.no_ensemble else ensemble_leg(args)
+    clo = None if args.no_closure else closure_leg(args)
     barrier_sync()
     e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     state_bytes = 11 * 4 * nodes
@@ -372,7 +429,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}", "l2": "state 830 MB > 126 MB L2, no flush needed",
                    "state_bytes": state_bytes},
         "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-        "precision_forms": forms, "ensemble": ens,
+        "precision_forms": forms, "ensemble": ens, "closure": clo,
         "clocks": clk, "check": {"mass": red["mass"], "umax": red["umax"], "mass_a": red["mass_a"]},
     }
     print(json.dumps(line), flush=True)
@@ -392,6 +449,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-precision-forms", action="store_true", help="skip the bf16 / fp16 storage legs")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-domain ensemble leg")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure jet leg")
     ap.add_argument("--nz", type=int, default=0, help="shallower channel (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -2,9 +2,10 @@
 
     python -m entropicthreadsafe_b200.build [--verbose]
 
-Each csrc/*.cu is compiled to an object under csrc/_build (in parallel),
-then linked into entropicthreadsafe_b200/libtslb.so with the static CUDA
-runtime.
+Each csrc/*.cu (and the host-only csrc/tslb_io.cpp) is compiled to an
+object under csrc/_build (in parallel), then linked into
+entropicthreadsafe_b200/libtslb.so with the static CUDA runtime; the host
+driver driver/tslb_run.cpp is linked against it as entropicthreadsafe_b200/tslb_run.
 """
 from __future__ import annotations
 
@@ -17,9 +18,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 OUT = os.path.join(HERE, "libtslb.so")
-SOURCES = ["tslb.cu", "closure.cu"]
+DRIVER_SRC = os.path.join(HERE, "driver", "tslb_run.cpp")
+DRIVER = os.path.join(HERE, "tslb_run")
+SOURCES = ["tslb.cu", "closure.cu", "tslb_io.cpp"]
 HEADERS = ["tslb_device.cuh", "tslb_step.cuh", "tslb_internal.h", "tcgen05.cuh", "closure_mlp.cuh"]
-INCLUDES = ["tslb.h", "tslb_closure.h"]
+INCLUDES = ["tslb.h", "tslb_closure.h", "tslb_io.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
@@ -32,10 +35,20 @@ def _deps() -> list:
 
 
 def _stale() -> bool:
-    if not os.path.exists(OUT):
+    if not os.path.exists(OUT) or not os.path.exists(DRIVER):
         return True
-    t = os.path.getmtime(OUT)
-    return any(os.path.getmtime(d) > t for d in _deps())
+    t = min(os.path.getmtime(OUT), os.path.getmtime(DRIVER))
+    return any(os.path.getmtime(d) > t for d in _deps() + [DRIVER_SRC])
+
+
+def build_driver() -> str:
+    """The host driver tslb_run (C++), linked against libtslb.so next to it."""
+    cxx = os.environ.get("CXX_DRIVER", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", "-o", DRIVER, DRIVER_SRC, "-L" + HERE, "-ltslb", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("driver build failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+    return DRIVER
 
 
 def _compile(src: str):
@@ -62,6 +75,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc link failed:\n" + " ".join(link) + "\n" + res.stdout + res.stderr)
+    build_driver()
     return OUT
 
 

@@ -200,8 +200,21 @@ def lib() -> ctypes.CDLL:
         L.tslb_stats_download.argtypes = [vp, ip, fp, fp, fp, fp, fp, lp]
         L.tslb_stats_download.restype = ip
         _declare_closure(L)
+        cp = ctypes.c_char_p
+        for name, args, res in (("tslb_write_raw", [cp, fp, ctypes.c_longlong], ip),
+                                ("tslb_write_vti", [cp, cp, ip, ip, ip, ip, fp], ip),
+                                ("tslb_write_slices", [cp, cp, ip, ip, ip, ip, fp], ip),
+                                ("tslb_frame_path", [ctypes.c_char_p, ip, cp, cp, cp, ip, cp], ip),
+                                ("tslb_checkpoint_save", [vp, cp], ip),
+                                ("tslb_checkpoint_load", [vp, cp], ip),
+                                ("tslb_steps_done", [vp], ctypes.c_longlong)):
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = res
         _lib = L
     return _lib
+
+
+DRIVER_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tslb_run")
 
 
 def fptr(a: np.ndarray):

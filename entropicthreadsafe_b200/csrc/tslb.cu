@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/tslb.h"
+#include "../../include/tslb_io.h"
 #include "tslb_internal.h"
 #include "tslb_step.cuh"
 
@@ -815,6 +816,89 @@ const char* tslb_last_error(tslb_ctx* c) {
 }
 
 }  // extern "C"
+
+// ---- checkpoints (include/tslb_io.h) ----
+namespace {
+struct CkptHeader {
+    char magic[8];
+    int32_t version, nx, ny, nz, mode, precision, esize, nfields;
+    long long steps_done;
+    float scale[NF];
+    tslb_params params;
+};
+const char kCkptMagic[8] = {'T', 'S', 'L', 'B', 'C', 'K', 'P', '1'};
+}  // namespace
+
+extern "C" {
+
+long long tslb_steps_done(tslb_ctx* c) { return c ? c->steps_done : 0; }
+
+int tslb_checkpoint_save(tslb_ctx* c, const char* path) {
+    if (!c || !path) return fail(c, TSLB_ERR_ARG, "tslb_checkpoint_save: NULL");
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "tslb_checkpoint_save before an upload");
+    CkptHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1; h.nx = c->nx; h.ny = c->ny; h.nz = c->nz; h.mode = c->p.mode; h.precision = c->p.precision;
+    h.esize = c->esize; h.nfields = NF; h.steps_done = c->steps_done;
+    for (int f = 0; f < NF; ++f) h.scale[f] = c->scale[f];
+    h.params = c->p;
+    std::vector<char> buf((size_t)c->esize * c->n);
+    FILE* fh = std::fopen(path, "wb");
+    if (!fh) return fail(c, TSLB_ERR_ARG, std::string("tslb_checkpoint_save: cannot open ") + path);
+    bool ok = std::fwrite(&h, sizeof(h), 1, fh) == 1;
+    for (int f = 0; f < NF && ok; ++f) {
+        const char* src = static_cast<const char*>(c->state[c->cur]) + (size_t)f * c->N * c->esize;
+        cudaError_t e = cudaMemcpyAsync(buf.data(), src, buf.size(), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            std::fclose(fh);
+            return fail(c, TSLB_ERR_CUDA, std::string("tslb_checkpoint_save: ") + cudaGetErrorString(e));
+        }
+        ok = std::fwrite(buf.data(), 1, buf.size(), fh) == buf.size();
+    }
+    if (std::fclose(fh) != 0 || !ok) return fail(c, TSLB_ERR_ARG, std::string("tslb_checkpoint_save: write failed: ") + path);
+    return TSLB_OK;
+}
+
+int tslb_checkpoint_load(tslb_ctx* c, const char* path) {
+    if (!c || !path) return fail(c, TSLB_ERR_ARG, "tslb_checkpoint_load: NULL");
+    FILE* fh = std::fopen(path, "rb");
+    if (!fh) return fail(c, TSLB_ERR_ARG, std::string("tslb_checkpoint_load: cannot open ") + path);
+    CkptHeader h;
+    if (std::fread(&h, sizeof(h), 1, fh) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1 ||
+        h.nfields != NF) {
+        std::fclose(fh);
+        return fail(c, TSLB_ERR_ARG, "tslb_checkpoint_load: not a TSLB checkpoint");
+    }
+    if (h.nx != c->nx || h.ny != c->ny || h.nz != c->nz || h.mode != c->p.mode || h.precision != c->p.precision ||
+        h.esize != c->esize) {
+        std::fclose(fh);
+        return fail(c, TSLB_ERR_ARG, "tslb_checkpoint_load: sizes, mode or precision differ from the lattice's");
+    }
+    std::vector<char> buf((size_t)c->esize * c->n);
+    for (int f = 0; f < NF; ++f) {
+        if (std::fread(buf.data(), 1, buf.size(), fh) != buf.size()) {
+            std::fclose(fh);
+            return fail(c, TSLB_ERR_ARG, "tslb_checkpoint_load: truncated file");
+        }
+        char* dst = static_cast<char*>(c->state[c->cur]) + (size_t)f * c->N * c->esize;
+        cudaError_t e = cudaMemcpyAsync(dst, buf.data(), buf.size(), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            std::fclose(fh);
+            return fail(c, TSLB_ERR_CUDA, std::string("tslb_checkpoint_load: ") + cudaGetErrorString(e));
+        }
+    }
+    std::fclose(fh);
+    for (int f = 0; f < NF; ++f) c->scale[f] = h.scale[f];
+    c->steps_done = h.steps_done;
+    c->loaded = true;
+    return TSLB_OK;
+}
+
+}  // extern "C"
+
 
 // ------------------------------------------------- step without allocation
 // Scratch of tslb_step_noalloc: a fixed device array of this file.  In host

@@ -100,6 +100,17 @@ class Lattice:
         self._check(self.L.tslb_download_tau_correction(self.h, capi.fptr(out)))
         return out
 
+    # -- checkpoints (include/tslb_io.h) --------------------------------
+    def checkpoint_save(self, path: str) -> None:
+        self._check(self.L.tslb_checkpoint_save(self.h, str(path).encode()))
+
+    def checkpoint_load(self, path: str) -> None:
+        self._check(self.L.tslb_checkpoint_load(self.h, str(path).encode()))
+
+    @property
+    def steps_done(self) -> int:
+        return int(self.L.tslb_steps_done(self.h))
+
     # -- time averages ---------------------------------------------------
     def stats_reset(self) -> None:
         self._check(self.L.tslb_stats_reset(self.h))

@@ -9,7 +9,7 @@ import pytest
 from entropicthreadsafe_b200 import capi
 
 INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
-HEADERS = ("tslb.h", "tslb_closure.h")
+HEADERS = tuple(sorted(h for h in os.listdir(INCLUDE) if h.endswith(".h")))
 
 
 def declared_symbols():
