@@ -49,6 +49,22 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(ms: float, device: str = "cuda") -> float:
+    """Device time of the slowest rank (every rank calls this, in the same order)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(ws: int, nodes: int, steps: int, ms_max: float) -> float:
+    """Weak scaling: every rank advances its own replica of `nodes` nodes."""
+    return ws * nodes * steps / (ms_max * 1e-3) / 1e6
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -367,13 +383,8 @@ def run_ours(args):
     clk = clocks.stop()
     barrier_sync()
     red = lat.reduce()
-    ms_max = ms
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = ws * nodes * args.steps / (ms_max * 1e-3) / 1e6
+    ms_max = max_over_ranks(ms)
+    value = whole_job_mlups(ws, nodes, args.steps, ms_max)
     ms_step = ms_max / args.steps
     # ---- precision forms of the same workload (bf16, fp16 with per-field scale) ----
     forms = None
