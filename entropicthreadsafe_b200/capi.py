@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libtslb.so")
 
 # ---- constants mirrored from include/tslb.h ----
 OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(7)
-MODE_PHASEFIELD, MODE_COLOUR = 0, 1
+MODE_PHASEFIELD, MODE_COLOUR, MODE_SINGLE = 0, 1, 2
 PREC_FP32, PREC_BF16, PREC_FP16S = 0, 1, 2
 BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET, BC_PRESSURE = range(6)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)

@@ -9,6 +9,7 @@ coarse jet (boundary_cds_3D_module.f90:862-1119) runs with the plain tau.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -167,6 +168,26 @@ class Closure:
         hist = np.empty(max(steps, 1), np.float32)
         self._check(self.L.tslb_closure_train(self.h, int(steps), int(batch), float(lr), int(seed), capi.fptr(hist)))
         return hist[:steps]
+
+
+TRAINED_JET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "closure_jet_192.npz")
+
+
+def load_trained(path: str = TRAINED_JET) -> dict:
+    """A trained network: params, mu, sd, dtau_max and the calibrated output
+    gain.  The packaged file is the network of the round-jet study
+    (closure_study: trained on box-filtered 384 x 384 x 768 runs, gain chosen
+    a posteriori on coarse 192 x 192 x 384 runs)."""
+    d = np.load(path)
+    return {k: d[k] for k in d.files}
+
+
+def trained_closure(path: str = TRAINED_JET) -> "Closure":
+    """A Closure loaded with a trained network, its output scaled by the calibrated gain."""
+    t = load_trained(path)
+    c = Closure()
+    c.set_params(t["params"], t["mu"], t["sd"], float(t["dtau_max"]) * float(t["gain"]))
+    return c
 
 
 def lattice_attach(lat: Lattice, closure: Closure | None, interval: int = 1) -> None:

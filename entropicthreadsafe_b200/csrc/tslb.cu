@@ -51,7 +51,9 @@ int validate(const tslb_params* p, int nx, int ny, int nz, std::string& why) {
     if (!p) { why = "params is NULL"; return TSLB_ERR_ARG; }
     if (nx < 1 || ny < 1 || nz < 1) { why = "sizes must be >= 1"; return TSLB_ERR_ARG; }
     if ((long long)nx * ny * nz > (1LL << 36)) { why = "lattice too large"; return TSLB_ERR_ARG; }
-    if (p->mode != TSLB_MODE_PHASEFIELD && p->mode != TSLB_MODE_COLOUR) { why = "unknown mode"; return TSLB_ERR_ARG; }
+    if (p->mode != TSLB_MODE_PHASEFIELD && p->mode != TSLB_MODE_COLOUR && p->mode != TSLB_MODE_SINGLE) {
+        why = "unknown mode"; return TSLB_ERR_ARG;
+    }
     if (p->precision != TSLB_PREC_FP32 && p->precision != TSLB_PREC_BF16 && p->precision != TSLB_PREC_FP16S) {
         why = "unknown precision"; return TSLB_ERR_ARG;
     }
@@ -173,8 +175,10 @@ __global__ void pops_to_moments_kernel(int nx, int ny, int nz, long long N, int 
     for (int q = 0; q < 27; ++q) { tot[q] = f[q * vol + h]; ra += tot[q]; }
     if (colour) {
         for (int q = 0; q < 27; ++q) { float gb = g[q * vol + h]; rb += gb; tot[q] += gb; }
-    } else {
+    } else if (g) {
         for (int q = 0; q < 7; ++q) phi += g[q * vol + h];
+    } else {
+        phi = 1.f;   // single component
     }
     const float rho = colour ? ra + rb : ra;
     if (colour) phi = (ra - rb) / rho;
@@ -341,6 +345,8 @@ cudaError_t set_step_attributes() {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, T>, attr, sc);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true, T>, attr, sp);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false, T>, attr, sp);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, true, T>, attr, sp);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, false, T>, attr, sp);
     };
     one(float{});
     one(__nv_bfloat16{});
@@ -378,6 +384,9 @@ void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) 
         } else if (mode == TSLB_MODE_COLOUR) {
             if (vec) step_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, st>>>(a);
             else step_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, st>>>(a);
+        } else if (mode == TSLB_MODE_SINGLE) {
+            if (vec) step_kernel<TSLB_MODE_SINGLE, true, T><<<grid, block, sm, st>>>(a);
+            else step_kernel<TSLB_MODE_SINGLE, false, T><<<grid, block, sm, st>>>(a);
         } else {
             if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true, T><<<grid, block, sm, st>>>(a);
             else step_kernel<TSLB_MODE_PHASEFIELD, false, T><<<grid, block, sm, st>>>(a);
@@ -442,6 +451,16 @@ int fp32_view(tslb_ctx* c, const float** out) {
     int rc = state_to_io(c);
     *out = c->io;
     return rc;
+}
+
+// single-component mode: phi is held at 1 and the step does not write it,
+// so both ping-pong buffers carry the same phi field
+int single_phi_both(tslb_ctx* c) {
+    if (c->p.mode != TSLB_MODE_SINGLE) return TSLB_OK;
+    const size_t off = (size_t)F_PHI * c->N * c->esize, bytes = (size_t)c->n * c->esize;
+    CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(c->state[c->cur ^ 1]) + off, static_cast<char*>(c->state[c->cur]) + off,
+                                bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return TSLB_OK;
 }
 
 int ensure_dtau(tslb_ctx* c) {
@@ -557,6 +576,12 @@ int tslb_upload_moments(tslb_ctx* c, const float* rho, const float* u, const flo
                         const float* pyz, const float* pzz, const float* phi) {
     if (!c) return TSLB_ERR_ARG;
     const float* src[NF] = {rho, u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi};
+    std::vector<float> ones;
+    if (c->p.mode == TSLB_MODE_SINGLE) {
+        // single component: phi is held at 1 (the argument may be NULL)
+        ones.assign((size_t)c->n, 1.0f);
+        src[F_PHI] = ones.data();
+    }
     for (int f = 0; f < NF; ++f)
         if (!src[f]) return fail(c, TSLB_ERR_ARG, "tslb_upload_moments: NULL field");
     const bool fp32 = c->p.precision == TSLB_PREC_FP32;
@@ -586,6 +611,8 @@ int tslb_upload_moments(tslb_ctx* c, const float* rho, const float* u, const flo
         int rc = io_to_state(c);
         if (rc) return rc;
     }
+    int rc = tslb_internal::single_phi_both(c);
+    if (rc) return rc;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->loaded = true;
     return TSLB_OK;
@@ -593,15 +620,16 @@ int tslb_upload_moments(tslb_ctx* c, const float* rho, const float* u, const flo
 
 int tslb_upload_pops(tslb_ctx* c, const float* f, const float* g) {
     if (!c) return TSLB_ERR_ARG;
-    if (!f || !g) return fail(c, TSLB_ERR_ARG, "tslb_upload_pops: NULL populations");
+    const bool single = c->p.mode == TSLB_MODE_SINGLE;
+    if (!f || (!g && !single)) return fail(c, TSLB_ERR_ARG, "tslb_upload_pops: NULL populations");
     const long long vol = (long long)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
     const int nqg = c->p.mode == TSLB_MODE_COLOUR ? 27 : 7;
     float *df = nullptr, *dg = nullptr;
     CUDA_TRY(c, cudaMalloc(&df, sizeof(float) * 27 * vol));
-    cudaError_t e = cudaMalloc(&dg, sizeof(float) * nqg * vol);
+    cudaError_t e = single ? cudaSuccess : cudaMalloc(&dg, sizeof(float) * nqg * vol);
     if (e != cudaSuccess) { cudaFree(df); return fail(c, TSLB_ERR_CUDA, std::string("cudaMalloc(g): ") + cudaGetErrorString(e)); }
     e = cudaMemcpyAsync(df, f, sizeof(float) * 27 * vol, cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dg, g, sizeof(float) * nqg * vol, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && !single) e = cudaMemcpyAsync(dg, g, sizeof(float) * nqg * vol, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
         const int bs = 128;
         const bool fp32 = c->p.precision == TSLB_PREC_FP32;
@@ -614,6 +642,7 @@ int tslb_upload_pops(tslb_ctx* c, const float* f, const float* g) {
             default_scales(c);
             if (io_to_state(c) != TSLB_OK) e = cudaGetLastError();
         }
+        if (e == cudaSuccess && tslb_internal::single_phi_both(c) != TSLB_OK) e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(df);
@@ -893,6 +922,9 @@ int tslb_checkpoint_load(tslb_ctx* c, const char* path) {
     std::fclose(fh);
     for (int f = 0; f < NF; ++f) c->scale[f] = h.scale[f];
     c->steps_done = h.steps_done;
+    int rc = tslb_internal::single_phi_both(c);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->loaded = true;
     return TSLB_OK;
 }
@@ -1143,6 +1175,8 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
     for (int i = 1; i < n; ++i)
         if (params[i].mode != params[0].mode || params[i].precision != params[0].precision)
             return efail(nullptr, TSLB_ERR_ARG, "tslb_ensemble_create: members must share mode and precision");
+    if (params[0].mode == TSLB_MODE_SINGLE)
+        return efail(nullptr, TSLB_ERR_UNSUPPORTED, "tslb_ensemble_create: single-component members are not supported");
     for (int i = 0; i < n; ++i)
         for (int f = 0; f < 6; ++f)
             if (params[i].bc[f] == TSLB_BC_INLET)

@@ -264,6 +264,12 @@ __device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, co
         nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;
         A = iface ? a.acoef * a.sigma * omega : 0.f;
         U = u; V = v; W = w;
+    } else if (MODE == TSLB_MODE_SINGLE) {
+        // fused_TSLB_force_1c: equilibrium at the shifted velocity u + F
+        omega = a.omega_pf;
+        U = u + a.force[0];
+        V = v + a.force[1];
+        W = w + a.force[2];
     } else {
         omega = a.omega_pf;
         const long long id = nidx(a, x, y, z);
@@ -331,7 +337,7 @@ __device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, co
         // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta; n = 0 off the interface)
         const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
         K[K_C0] = phi; K[K_C1] = bb * nx_; K[K_C2] = bb * ny_; K[K_C3] = bb * nz_; K[K_C4] = d0;
-    } else {
+    } else if (MODE == TSLB_MODE_PHASEFIELD) {
         // D3Q7 phase field: g_q = G0 + e_q.G1 (recursive_2c_TSLB3D.f90:808-831)
         const float sh = 0.125f * a.sharp * phi * (1.f - phi);
         K[K_C0] = 0.125f * phi;

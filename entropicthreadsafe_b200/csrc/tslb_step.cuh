@@ -28,9 +28,12 @@ namespace tslb {
 
 // Coefficients live in shared memory as NCOEF scalar planes of CAREA floats
 // (slot-major), so each source loads exactly the slots its directions use.
+// (single-component mode has no colour slots)
+template <int MODE>
 __device__ __forceinline__ void store_coefs(float* dst, const float* K) {
+    constexpr int n = MODE == TSLB_MODE_SINGLE ? K_C0 : NCOEF;
 #pragma unroll
-    for (int c = 0; c < NCOEF; ++c) dst[c * CAREA] = K[c];
+    for (int c = 0; c < n; ++c) dst[c * CAREA] = K[c];
 }
 
 // P' = Q0 + cz Q1 + cz^2 Q2 of the directions (CXv, CYv, cz), cz = -1, 0, 1,
@@ -132,7 +135,7 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
             // colour is the target's own, so it adds no colour increment
             acc0[A_RHO] += sz.L(K_C4);
         }
-    } else {
+    } else if (MODE == TSLB_MODE_PHASEFIELD) {
         // phase field g (D3Q7): axis directions and the rest population
         if (CYv == 0) {
             const float g0 = sz.L(K_C0), gz = sz.L(K_C3);
@@ -154,7 +157,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                                 float* acc) {
     float Kp[NCOEF];
 #pragma unroll
-    for (int c = 0; c < NCOEF; ++c) Kp[c] = Kc[c * CAREA];
+    for (int c = 0; c < (MODE == TSLB_MODE_SINGLE ? (int)K_C0 : NCOEF); ++c) Kp[c] = Kc[c * CAREA];
     // colour mode accumulates colour increments over the target's own phi
     const float pht = Kp[K_C0];
     // own raw moments (velocity faces only)
@@ -198,7 +201,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                 // the reflected population carries the target's own colour: only the recolouring term
                 const float bc = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
                 acc[A_COL] += wq * invlen(c2) * bc;
-            } else if (c2 == 1) {
+            } else if (MODE == TSLB_MODE_PHASEFIELD && c2 == 1) {
                 const float ge = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
                 acc[A_COL] += Kp[K_C0] + ge;
             }
@@ -268,7 +271,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             if (MODE == TSLB_MODE_COLOUR) {
                 const float dphi = phib - pht;
                 acc[A_COL] += wq * fmaf(dphi, P, dphi);
-            } else if (c2 == 1) {
+            } else if (MODE == TSLB_MODE_PHASEFIELD && c2 == 1) {
                 // g entering from the face (:984-986, :1044-1045)
                 const float eu = dx * Ub[0] + dy * Ub[1] + dz * Ub[2];
                 acc[A_COL] += 0.125f * phib * (1.f + 3.f * eu);
@@ -569,14 +572,16 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                     if constexpr (std::is_same<T, __half>::value) {
                         g[0] *= a.iscale[F_PHI]; g[1] *= a.iscale[F_PHI]; g[2] *= a.iscale[F_PHI];
                     }
-                } else {
+                } else if (MODE == TSLB_MODE_PHASEFIELD) {
                     m[F_PHI] = ld_field<T>(a, F_PHI, (long long)gz * plane + nd.off);
                     gx = nd.off % a.nx;
                     gy = nd.off / a.nx;
+                } else {
+                    m[F_PHI] = 1.f;
                 }
                 node_coefs<MODE, TAU>(a, m, g, gx, gy, gz, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
-            store_coefs(coef + ci, K);
+            store_coefs<MODE>(coef + ci, K);
         }
         cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
@@ -622,8 +627,10 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 o[F_PHI] = MODE == TSLB_MODE_COLOUR ? fmaf(accm[A_COL], inv, phm) : accm[A_COL];
                 T* po = gout + (long long)t * plane + cn0.off;
                 float chk = 0.f;
+                // single-component mode does not step phi (held at 1 in both buffers)
+                constexpr int nout = MODE == TSLB_MODE_SINGLE ? F_PHI : NF;
 #pragma unroll
-                for (int f = 0; f < NF; ++f) {
+                for (int f = 0; f < nout; ++f) {
                     const T st = cvt_out<T>(o[f], a, f);
                     po[f * a.N] = st;
                     chk += Stor<T>::ld(st);

@@ -65,6 +65,11 @@ extern "C" {
                                     (recursive_2c_TSLB3D.f90); phi in [0,1]          */
 #define TSLB_MODE_COLOUR      1  /* colour gradient: perturbation + recolouring
                                     (recursive_colorTSLB3D.f90); phi in [-1,1]       */
+#define TSLB_MODE_SINGLE      2  /* single component (fused_TSLB_1c / fused_TSLB_force_1c,
+                                    TSLB_2C-mpi/lb_kernels_module.f90:414-736): the f
+                                    step of the phase-field mode with no phase field,
+                                    force as the velocity shift u + F of the equilibrium;
+                                    phi is held at 1 and not stepped; tau = tau_a    */
 
 /* ---- storage precision of the device moment state ---- */
 #define TSLB_PREC_FP32        0

@@ -109,6 +109,41 @@ def test_colour_jet_inlet_pressure_outlet():
     assert abs(float(np.mean(o64["rho"][-1])) - 1.0) < 2e-3
 
 
+def single_component_case(nx, ny, nz, seed, bc, bc_u, force):
+    rng = np.random.default_rng(seed)
+    p = capi.make_params(mode=capi.MODE_SINGLE, tau_a=0.6, force=force, bc=bc, bc_u=bc_u)
+    f = workloads.empty_fields(nx, ny, nz)
+    for k in ("u", "v", "w"):
+        f[k][:] = rng.normal(0, 0.02, f[k].shape)
+    for k in ("pxx", "pxy", "pxz", "pyy", "pyz", "pzz"):
+        f[k][:] = rng.normal(0, 1e-4, f[k].shape)
+    f["rho"][:] = 1.0 + rng.normal(0, 1e-3, f["rho"].shape)
+    f["phi"][:] = 1.0
+    return p, f
+
+
+@pytest.mark.parametrize("walls", ["periodic", "bounceback_and_moving_wall"])
+def test_single_component_matches_oracle(walls):
+    """Single-component mode against the phase-field oracle with phi = 1,
+    which is the reference's fused_TSLB_force_1c."""
+    if walls == "periodic":
+        bc, bcu = [capi.BC_PERIODIC] * 6, [[0, 0, 0]] * 6
+    else:
+        bc = [capi.BC_PERIODIC] * 4 + [capi.BC_BOUNCEBACK, capi.BC_VELOCITY]
+        bcu = [[0, 0, 0]] * 5 + [[0.03, 0.0, 0.0]]
+    p, f = single_component_case(20, 18, 24, 3, bc, bcu, (1e-5, 2e-6, 0.0))
+    gpu, _ = run_gpu(p, f, 100)
+    o64, _ = run_oracle(p, f, 100, fp64=True)
+    o32, _ = run_oracle(p, f, 100, fp64=False)
+    assert np.all(gpu["phi"] == 1.0)
+    for k in ("phi",):
+        gpu.pop(k); o64.pop(k); o32.pop(k)
+    eg = {k: rel_err(gpu[k], o64[k]) for k in gpu}
+    e32 = {k: rel_err(o32[k], o64[k]) for k in gpu}
+    bad = {k: (eg[k], e32[k]) for k in eg if eg[k] > max(TARGET, TOL_FACTOR * e32[k])}
+    assert not bad, bad
+
+
 def test_phasefield_droplet_bounceback_all_faces():
     n = 20
     p = capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=0.7, sigma=0.01, sharp_c=0.9,

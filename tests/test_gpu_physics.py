@@ -95,3 +95,19 @@ def test_couette_profile():
     lin = np.polyval(slope, z)
     assert np.abs(u - lin).max() < 2e-3 * U  # linear profile
     assert slope[0] > 0 and abs(u[-1] - U) < 0.1 * U and abs(u[0] + U) < 0.1 * U
+
+
+def test_single_component_poiseuille_profile():
+    """Single-component mode (the reference's fused_TSLB_force_1c): the
+    force-driven channel between bounce-back walls reaches u(z) = g z (H - z)/(2 nu)."""
+    H, tau, g = 24, 1.0, 1e-6
+    nu = (tau - 0.5) / 3
+    bc = [capi.BC_PERIODIC] * 4 + [capi.BC_BOUNCEBACK] * 2
+    p = capi.make_params(mode=capi.MODE_SINGLE, tau_a=tau, force=(g, 0.0, 0.0), bc=bc)
+    f = workloads.empty_fields(8, 8, H)
+    _, _, out = run(p, f, 12000)
+    u = out["u"].mean(axis=(1, 2)).astype(np.float64)
+    z = np.arange(H) + 0.5
+    exact = g / (2 * nu) * z * (H - z)
+    assert np.abs(u - exact).max() / exact.max() < 0.01
+    assert np.all(out["phi"] == 1.0)
