@@ -142,8 +142,8 @@ struct Oracle {
         : prm(p), nx(nx_), ny(ny_), nz(nz_), sx(nx_ + 2), sy(ny_ + 2), sz(nz_ + 2) {
         vol = size_t(sx) * sy * sz;
         colour = p.mode == TSLB_MODE_COLOUR;
-        // TSLB_MODE_SINGLE runs as the phase-field step with phi held at 1: with a uniform
-        // phi the CSF force vanishes and the f step is fused_TSLB_force_1c
+        // TSLB_MODE_SINGLE runs as the phase-field step: at sigma = 0 (or with a uniform
+        // phi) the CSF force vanishes and its f step is fused_TSLB_force_1c
         // (TSLB_2C-mpi/lb_kernels_module.f90:574-736)
         nq_g = colour ? 27 : 7;
         f.assign(27 * vol, R(0));

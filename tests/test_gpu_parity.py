@@ -111,7 +111,9 @@ def test_colour_jet_inlet_pressure_outlet():
 
 def single_component_case(nx, ny, nz, seed, bc, bc_u, force):
     rng = np.random.default_rng(seed)
-    p = capi.make_params(mode=capi.MODE_SINGLE, tau_a=0.6, force=force, bc=bc, bc_u=bc_u)
+    # sigma = 0: the oracle's phase-field step then has no CSF force whatever its
+    # phi does at the walls, and its f step is fused_TSLB_force_1c
+    p = capi.make_params(mode=capi.MODE_SINGLE, tau_a=0.6, sigma=0.0, force=force, bc=bc, bc_u=bc_u)
     f = workloads.empty_fields(nx, ny, nz)
     for k in ("u", "v", "w"):
         f[k][:] = rng.normal(0, 0.02, f[k].shape)
@@ -124,8 +126,8 @@ def single_component_case(nx, ny, nz, seed, bc, bc_u, force):
 
 @pytest.mark.parametrize("walls", ["periodic", "bounceback_and_moving_wall"])
 def test_single_component_matches_oracle(walls):
-    """Single-component mode against the phase-field oracle with phi = 1,
-    which is the reference's fused_TSLB_force_1c."""
+    """Single-component mode against the phase-field oracle at sigma = 0,
+    whose f step is the reference's fused_TSLB_force_1c."""
     if walls == "periodic":
         bc, bcu = [capi.BC_PERIODIC] * 6, [[0, 0, 0]] * 6
     else:
