@@ -338,6 +338,36 @@ def closure_leg(args):
     return res
 
 
+def single_leg(args):
+    """Single-component mode (the reference's fused_TSLB_force_1c) on the channel
+    384 x 192 x 128 without droplets: force gx, bounce-back walls at z; 80 B per
+    lattice update (10 moment fields read and written)."""
+    import torch
+    from entropicthreadsafe_b200 import capi, workloads
+    from entropicthreadsafe_b200.solver import Lattice
+    p, f = workloads.channel()
+    p.mode = capi.MODE_SINGLE
+    f["phi"][:] = 1.0
+    nz, ny, nx = f["rho"].shape
+    nodes = nx * ny * nz
+    with Lattice(p, nx, ny, nz) as lat:
+        st = torch.cuda.ExternalStream(lat.stream)
+        lat.upload_moments(f)
+        lat.step(args.warmup)
+        lat.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lat.step(args.steps)
+        e1.record(st)
+        lat.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+    peak, kind = peaks()
+    gbs = 80 * nodes / (ms * 1e-3) / 1e9
+    return {"workload": "channel 384x192x128, single component, gx 2.5e-6, bounce-back walls", "value": nodes / (ms * 1e-3) / 1e6,
+            "unit": UNIT, "ms_per_step": ms, "bytes_per_lu": 80,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -415,6 +445,7 @@ def run_ours(args):
         lat.close()
     ens = None if args.no_ensemble else ensemble_leg(args)
     clo = None if args.no_closure else closure_leg(args)
+    sgl = None if args.no_single else single_leg(args)
     barrier_sync()
     e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     state_bytes = 11 * 4 * nodes
@@ -440,7 +471,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}", "l2": "state 830 MB > 126 MB L2, no flush needed",
                    "state_bytes": state_bytes},
         "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-        "precision_forms": forms, "ensemble": ens, "closure": clo,
+        "precision_forms": forms, "ensemble": ens, "closure": clo, "single_component": sgl,
         "clocks": clk, "check": {"mass": red["mass"], "umax": red["umax"], "mass_a": red["mass_a"]},
     }
     print(json.dumps(line), flush=True)
@@ -461,6 +492,7 @@ def main():
     ap.add_argument("--no-precision-forms", action="store_true", help="skip the bf16 / fp16 storage legs")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-domain ensemble leg")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure jet leg")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-component channel leg")
     ap.add_argument("--nz", type=int, default=0, help="shallower channel (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -189,6 +189,8 @@ def lib() -> ctypes.CDLL:
         lp = ctypes.POINTER(ctypes.c_longlong)
         L.tslb_set_inlet_disc.argtypes = [vp, ip] + [ctypes.c_float] * 5 + [ctypes.c_ulonglong] * 2
         L.tslb_set_inlet_disc.restype = ip
+        L.tslb_set_solid_mask.argtypes = [vp, vp]
+        L.tslb_set_solid_mask.restype = ip
         L.tslb_set_tau_correction.argtypes = [vp, fp]
         L.tslb_set_tau_correction.restype = ip
         L.tslb_download_tau_correction.argtypes = [vp, fp]

@@ -1050,6 +1050,7 @@ int tslb_attach_closure(tslb_ctx* L, tslb_closure* c, int interval) {
     if (L->p.mode != TSLB_MODE_COLOUR || L->p.precision != TSLB_PREC_FP32)
         return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: colour mode with FP32 storage only");
     if (c->device != L->device) return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: closure and lattice on different devices");
+    if (L->solid_on) return tslb_internal::fail(L, TSLB_ERR_UNSUPPORTED, "tslb_attach_closure: not combined with solid nodes");
     int rc = tslb_internal::ensure_dtau(L);
     if (rc) return rc;
     // the first refresh sees the static correction as the previous total

@@ -119,11 +119,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait for phase `parity` to complete: gives up after about
-// `max_cycles` SM clock cycles and returns false.
+// `max_cycles` SM clock cycles and returns false.  Between polls the thread
+// sleeps briefly, so a waiting warp leaves its issue slots to the other
+// CTAs on the SM.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long max_cycles) {
+    if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
+    while (!mbar_try_wait(bar, parity)) {
         if (clock64() - t0 > max_cycles) return false;
+        __nanosleep(32);
+    }
     return true;
 }
 

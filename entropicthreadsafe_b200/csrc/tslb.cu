@@ -99,6 +99,8 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
     }
     a.flags = c->flags;
     a.dtau = c->closure ? c->dtau : (c->base_on ? c->dtau_base : nullptr);
+    a.solid = c->solid_on ? c->solid : nullptr;
+    a.near = c->solid_on ? c->near : nullptr;
     for (int f = 0; f < NF; ++f) {
         a.scale[f] = c->scale[f];
         a.iscale[f] = 1.0f / c->scale[f];
@@ -115,6 +117,7 @@ __global__ void normals_kernel(const StepArgs a, float* nrm) {
     const int x = (int)(i % a.nx), y = (int)((i / a.nx) % a.ny), z = (int)(i / ((long long)a.nx * a.ny));
     float g[3];
     grad_phi<T>(a, x, y, z, g);
+    if (a.solid && bit_at(a.solid, i)) g[0] = g[1] = g[2] = 0.f;   // normals of solid nodes are 0
     const float den = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + 1e-9f;
     nrm[i] = g[0] / den;
     nrm[a.N + i] = g[1] / den;
@@ -281,6 +284,45 @@ __global__ void inlet_disc_kernel(float* plane, int n0, int n1, int axis, float 
     plane[3 * pa + i] = in ? 1.0f : -1.0f;
 }
 
+// solid bit mask from isfluid bytes: word w holds nodes 32w .. 32w+31
+__global__ void solid_bits_kernel(const unsigned char* __restrict__ isfluid, long long n, unsigned int* solid) {
+    const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (w * 32 >= n) return;
+    unsigned int b = 0;
+    for (int k = 0; k < 32; ++k) {
+        const long long i = w * 32 + k;
+        if (i < n && isfluid[i] == 0) b |= 1u << k;
+    }
+    solid[w] = b;
+}
+
+// fluid nodes with a solid node among their 26 neighbours (periodic axes wrap;
+// a neighbour behind a non-periodic face is not an interior solid)
+__global__ void near_bits_kernel(const unsigned char* __restrict__ isfluid, int nx, int ny, int nz, int px, int py,
+                                 int pz, unsigned int* near) {
+    const long long n = (long long)nx * ny * nz;
+    const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (w * 32 >= n) return;
+    unsigned int b = 0;
+    for (int k = 0; k < 32; ++k) {
+        const long long i = w * 32 + k;
+        if (i >= n || isfluid[i] == 0) continue;
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+        bool hit = false;
+        for (int dz = -1; dz <= 1 && !hit; ++dz)
+            for (int dy = -1; dy <= 1 && !hit; ++dy)
+                for (int dx = -1; dx <= 1 && !hit; ++dx) {
+                    int sx = x + dx, sy = y + dy, sz = z + dz;
+                    if (sx < 0 || sx >= nx) { if (!px) continue; sx = (sx + nx) % nx; }
+                    if (sy < 0 || sy >= ny) { if (!py) continue; sy = (sy + ny) % ny; }
+                    if (sz < 0 || sz >= nz) { if (!pz) continue; sz = (sz + nz) % nz; }
+                    hit = isfluid[sx + (long long)nx * (sy + (long long)ny * sz)] == 0;
+                }
+        if (hit) b |= 1u << k;
+    }
+    near[w] = b;
+}
+
 // running sums of u, v, w, phi and w^2 (time averages of the jet statistics)
 __global__ void stats_accumulate_kernel(const float* __restrict__ s, long long n, long long N, float* __restrict__ acc) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -351,9 +393,16 @@ cudaError_t set_step_attributes() {
     one(float{});
     one(__nv_bfloat16{});
     one(__half{});
-    const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, 4);
+    const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, 4), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, 4);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, float, true>, attr, sc);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, float, true>, attr, sc);
+    // interior solids (FP32 storage)
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, float, false, true>, attr, sc);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, float, false, true>, attr, sc);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true>, attr, sp);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true>, attr, sp);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, true, float, false, true>, attr, sp);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, false, float, false, true>, attr, sp);
     return e;
 }
 
@@ -377,7 +426,19 @@ void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) 
         using T = decltype(tag);
         const bool vec = a.nx % (16 / (int)sizeof(T)) == 0;
         const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
-        if (mode == TSLB_MODE_COLOUR && a.dtau && std::is_same<T, float>::value) {
+        if (a.solid && std::is_same<T, float>::value) {
+            // interior solid nodes (FP32 storage, no tau correction; checked by tslb_set_solid_mask)
+            if (mode == TSLB_MODE_COLOUR) {
+                if (vec) step_kernel<TSLB_MODE_COLOUR, true, float, false, true><<<grid, block, sm, st>>>(a);
+                else step_kernel<TSLB_MODE_COLOUR, false, float, false, true><<<grid, block, sm, st>>>(a);
+            } else if (mode == TSLB_MODE_SINGLE) {
+                if (vec) step_kernel<TSLB_MODE_SINGLE, true, float, false, true><<<grid, block, sm, st>>>(a);
+                else step_kernel<TSLB_MODE_SINGLE, false, float, false, true><<<grid, block, sm, st>>>(a);
+            } else {
+                if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true><<<grid, block, sm, st>>>(a);
+                else step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true><<<grid, block, sm, st>>>(a);
+            }
+        } else if (mode == TSLB_MODE_COLOUR && a.dtau && std::is_same<T, float>::value) {
             // per-node tau correction (FP32 storage only; checked by the callers)
             if (vec) step_kernel<TSLB_MODE_COLOUR, true, float, true><<<grid, block, sm, st>>>(a);
             else step_kernel<TSLB_MODE_COLOUR, false, float, true><<<grid, block, sm, st>>>(a);
@@ -565,6 +626,8 @@ void tslb_destroy(tslb_ctx* c) {
     cudaFree(c->red);
     cudaFree(c->dtau);
     cudaFree(c->dtau_base);
+    cudaFree(c->solid);
+    cudaFree(c->near);
     cudaFree(c->stats);
     for (int f = 0; f < 6; ++f) cudaFree(c->inlet[f]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -751,8 +814,40 @@ int tslb_set_inlet_disc(tslb_ctx* c, int face, float c0, float c1, float radius,
     return TSLB_OK;
 }
 
+int tslb_set_solid_mask(tslb_ctx* c, const unsigned char* isfluid) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!isfluid) {
+        c->solid_on = false;
+        return TSLB_OK;
+    }
+    if (c->p.precision != TSLB_PREC_FP32)
+        return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_solid_mask: FP32 storage only");
+    if (c->base_on || c->closure)
+        return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_solid_mask: not combined with a tau correction or closure");
+    const long long words = (c->n + 31) / 32;
+    if (!c->solid) CUDA_TRY(c, cudaMalloc(&c->solid, sizeof(unsigned int) * words));
+    if (!c->near) CUDA_TRY(c, cudaMalloc(&c->near, sizeof(unsigned int) * words));
+    unsigned char* d = nullptr;
+    CUDA_TRY(c, cudaMalloc(&d, (size_t)c->n));
+    cudaError_t e = cudaMemcpyAsync(d, isfluid, (size_t)c->n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        const unsigned g = (unsigned)((words + 255) / 256);
+        solid_bits_kernel<<<g, 256, 0, c->stream>>>(d, c->n, c->solid);
+        near_bits_kernel<<<g, 256, 0, c->stream>>>(d, c->nx, c->ny, c->nz, c->p.bc[0] == TSLB_BC_PERIODIC,
+                                                  c->p.bc[2] == TSLB_BC_PERIODIC, c->p.bc[4] == TSLB_BC_PERIODIC, c->near);
+        c->launches += 2;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string("tslb_set_solid_mask: ") + cudaGetErrorString(e));
+    c->solid_on = true;
+    return TSLB_OK;
+}
+
 int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
     if (!c) return TSLB_ERR_ARG;
+    if (c->solid_on && dtau) return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_tau_correction: not combined with solid nodes");
     if (!dtau) {
         c->base_on = false;
         return TSLB_OK;

@@ -81,7 +81,13 @@ struct StepArgs {
     FaceBC face[6];
     unsigned int* flags;    // bit 0: non-finite moment produced
     const float* dtau;      // colour: per-node correction of tau (stride N), or null
+    const unsigned int* solid;  // interior solid nodes, one bit per node (bit i & 31 of word i >> 5), or null
+    const unsigned int* near;   // fluid nodes with a solid one among their 26 neighbours, same layout
 };
+
+__device__ __forceinline__ bool bit_at(const unsigned int* b, long long i) {
+    return (__ldg(b + (i >> 5)) >> (i & 31)) & 1u;
+}
 
 // Storage types of the moment state: FP32, BF16 or FP16 (scaled).  All
 // arithmetic is FP32; conversion happens on load and store.

@@ -37,6 +37,11 @@ struct tslb_ctx {
     float* dtau = nullptr;
     float* dtau_base = nullptr;
     bool base_on = false;
+    // interior solid nodes (tslb_set_solid_mask): bit masks of solid nodes and
+    // of fluid nodes with a solid neighbour
+    unsigned int* solid = nullptr;
+    unsigned int* near = nullptr;
+    bool solid_on = false;
     tslb_closure* closure = nullptr;       // attached closure (not owned)
     int closure_interval = 1;
     long long steps_done = 0;

@@ -152,7 +152,7 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 
 // Regularized or bounce-back populations entering target (x,y,z) from
 // behind non-periodic faces; Kp points at the target's own coefficients.
-template <int MODE, class T, bool TAU = false>
+template <int MODE, class T, bool TAU = false, bool SOLID = false>
 __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y, int z,
                                 float* acc) {
     float Kp[NCOEF];
@@ -182,16 +182,25 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                 if (k == TSLB_BC_VELOCITY || k == TSLB_BC_INLET || k == TSLB_BC_OUTLET || k == TSLB_BC_PRESSURE) vface = f;
             }
         }
-        if (!solid) continue;
+        // an interior solid source node (the lattice's solid mask), periodic axes wrapped
+        bool msolid = false;
+        if (SOLID && !solid) {
+            const int sx = x - dx, sy = y - dy, sz = z - dz;
+            msolid = bit_at(a.solid, nidx(a, sx < 0 ? sx + a.nx : (sx >= a.nx ? sx - a.nx : sx),
+                                          sy < 0 ? sy + a.ny : (sy >= a.ny ? sy - a.ny : sy),
+                                          sz < 0 ? sz + a.nz : (sz >= a.nz ? sz - a.nz : sz)));
+        }
+        if (!solid && !msolid) continue;
         const int c2 = dx * dx + dy * dy + dz * dz;
         const float wq = wclass(c2);
         if (MODE == TSLB_MODE_COLOUR) {
             // The pull skips whole solid z planes, but a source behind an x or y
-            // face is a zero-coefficient node that added w (0 - phi_t): undo it.
+            // face, or an interior solid node, is a zero-coefficient node that
+            // added w (0 - phi_t): undo it.
             const bool xy_solid = (dx && (mask & (1u << (dx > 0 ? 0 : 1)))) || (dy && (mask & (1u << (dy > 0 ? 2 : 3))));
             const int sz = z - dz;
             const bool zplane_solid = a.face[4].kind != TSLB_BC_PERIODIC && (sz < 0 || sz >= a.nz);
-            if (xy_solid && !zplane_solid) acc[A_COL] += wq * pht;
+            if ((xy_solid && !zplane_solid) || msolid) acc[A_COL] += wq * pht;
         }
         if (vface < 0) {
             // half-way bounce-back: f_c(x) = f^post_{-c}(x)
@@ -369,7 +378,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // VEC: nx is a multiple of the 16-byte chunk, so chunks never straddle the
 // x faces and planes are staged with 16-byte cp.async copies.
 // One block's work: tile (bx, by) of columns and z chunk bz of lattice a.
-template <int MODE, bool VEC, class T, bool TAU = false>
+// SOLID: the lattice has interior solid nodes (bit masks a.solid, a.near).
+template <int MODE, bool VEC, class T, bool TAU = false, bool SOLID = false>
 __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, int bz) {
     using G = Geo<sizeof(T)>;
     constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
@@ -553,7 +563,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
             const int ci = r ? ci1 : ci0;
             const int mi = r ? mi1 : mi0;
             float K[NCOEF];
-            if (nd.out) {
+            // solid nodes (behind a face, or interior solids) send nothing
+            if (nd.out || (SOLID && bit_at(a.solid, (long long)gz * plane + nd.off))) {
 #pragma unroll
                 for (int c = 0; c < NCOEF; ++c) K[c] = 0.f;
             } else {
@@ -606,7 +617,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 unsigned mask = colmask;
                 if (!zper && s == 0) mask |= 16u;
                 if (!zper && s == a.nz - 1) mask |= 32u;
-                if (mask) boundary_target<MODE, T, TAU>(a, Kc, mask, X, Y, s, acc0);
+                const bool near_solid = SOLID && bit_at(a.near, (long long)s * plane + cn0.off);
+                if (mask || near_solid) boundary_target<MODE, T, TAU, SOLID>(a, Kc, mask, X, Y, s, acc0);
             }
             // ---- 4. target plane s-1 is complete ----
             const int t = s - 1;
@@ -626,6 +638,12 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 // colour mode: phi_t + (colour increment) / rho
                 o[F_PHI] = MODE == TSLB_MODE_COLOUR ? fmaf(accm[A_COL], inv, phm) : accm[A_COL];
                 T* po = gout + (long long)t * plane + cn0.off;
+                if (SOLID && bit_at(a.solid, (long long)t * plane + cn0.off)) {
+                    // interior solid nodes keep their moments
+                    const T* pi = gin + (long long)t * plane + cn0.off;
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) po[f * a.N] = pi[f * a.N];
+                } else {
                 float chk = 0.f;
                 // single-component mode does not step phi (held at 1 in both buffers)
                 constexpr int nout = MODE == TSLB_MODE_SINGLE ? F_PHI : NF;
@@ -636,6 +654,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                     chk += Stor<T>::ld(st);
                 }
                 if (!isfinite(chk)) atomicOr(a.flags, 1u);
+                }
             }
         }
         // rotate the target slots
@@ -646,9 +665,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     cp_async_wait<0>();
 }
 
-template <int MODE, bool VEC, class T, bool TAU = false>
+template <int MODE, bool VEC, class T, bool TAU = false, bool SOLID = false>
 __global__ void __launch_bounds__(NTHR, 2) step_kernel(const StepArgs a) {
-    step_block<MODE, VEC, T, TAU>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+    step_block<MODE, VEC, T, TAU, SOLID>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Work item of the ensemble kernel: lattice, tile column, z chunk.

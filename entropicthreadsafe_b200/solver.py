@@ -87,6 +87,14 @@ class Lattice:
         """Jet inlet drawn on the device (see tslb_set_inlet_disc; workloads.inlet_disc is its host mirror)."""
         self._check(self.L.tslb_set_inlet_disc(self.h, face, c0, c1, radius, speed, amp, int(seed), int(counter)))
 
+    def set_solid_mask(self, isfluid) -> None:
+        """Interior solid nodes: isfluid (nz, ny, nx), 1 fluid / 0 solid, or None."""
+        if isfluid is None:
+            self._check(self.L.tslb_set_solid_mask(self.h, None))
+            return
+        m = np.ascontiguousarray(isfluid, np.uint8).reshape(self.shape)
+        self._check(self.L.tslb_set_solid_mask(self.h, m.ctypes.data))
+
     def set_tau_correction(self, dtau) -> None:
         """Per-node relaxation-time correction (nz, ny, nx), or None to switch it off."""
         if dtau is None:

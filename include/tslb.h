@@ -176,6 +176,18 @@ int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
  * four planes (u, v, w, phi) of the face's extent, Fortran order. */
 int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
 
+/* Interior solid nodes: isfluid holds nx*ny*nz bytes (Fortran order), 1 for
+ * a fluid node and 0 for a solid one, as the reference's isfluid array
+ * (recursive_2c_TSLB3D.f90:79-85); NULL removes them.  Populations that
+ * would leave a fluid node toward a solid one come back to it (half-way
+ * bounce-back, boundary_cds_3D_module.f90:10-76 applied at every
+ * isfluid == 0 node), solid nodes keep their moments (their phi is the wall
+ * value the colour gradient and the phase field see), and phase-field
+ * normals at solid nodes are 0.  Face conditions apply as before; a source
+ * behind a face follows the face.  FP32 storage; not combined with a tau
+ * correction or a closure. */
+int  tslb_set_solid_mask(tslb_ctx* ctx, const unsigned char* isfluid);
+
 /* Jet inlet drawn on the device (asynchronous, no host copy): the plane of
  * inlet face `face` becomes a disc of radius `radius` centred at in-plane
  * coordinates (c0, c1) -- (x, y) for z faces, (x, z) for y faces, (y, z)

@@ -49,6 +49,8 @@ def _lib(fast: bool = False) -> ctypes.CDLL:
         lib.orc_set_pops.restype = ip
         lib.orc_set_inlet.argtypes = [vp, ip, dp]
         lib.orc_set_inlet.restype = ip
+        lib.orc_set_isfluid.argtypes = [vp, vp]
+        lib.orc_set_isfluid.restype = ip
         lib.orc_set_dtau.argtypes = [vp, dp]
         lib.orc_set_dtau.restype = ip
         lib.orc_step.argtypes = [vp, ip]
@@ -112,6 +114,14 @@ class Oracle:
     def set_inlet(self, face: int, planes: np.ndarray) -> None:
         planes = np.ascontiguousarray(planes, np.float64)
         self._check(self.lib.orc_set_inlet(self.h, face, _dptr(planes)))
+
+    def set_isfluid(self, isfluid) -> None:
+        """Interior solid nodes: isfluid (nz, ny, nx), 1 fluid / 0 solid, or None."""
+        if isfluid is None:
+            self._check(self.lib.orc_set_isfluid(self.h, None))
+            return
+        m = np.ascontiguousarray(isfluid, np.uint8).reshape(self.shape)
+        self._check(self.lib.orc_set_isfluid(self.h, m.ctypes.data))
 
     def set_tau_correction(self, dtau) -> None:
         """Per-node correction of the colour-mode relaxation time, (nz, ny, nx), or None."""

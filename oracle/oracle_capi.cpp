@@ -110,6 +110,13 @@ int orc_set_inlet(void* hp, int face, const double* in) {
     ORC_DISPATCH(hp, set_inlet_t(o, face, in));
 }
 int orc_set_dtau(void* hp, const double* in) { ORC_DISPATCH(hp, set_dtau_t(o, in)); }
+int orc_set_isfluid(void* hp, const unsigned char* in) {
+    ORC_DISPATCH(hp, (([&]() {
+        if (!in) { o.isfluid.clear(); return int(TSLB_OK); }
+        o.isfluid.assign(in, in + size_t(o.nx) * o.ny * o.nz);
+        return int(TSLB_OK);
+    })()));
+}
 int orc_step(void* hp, int nsteps) {
     ORC_DISPATCH(hp, (([&]() { for (int s = 0; s < nsteps; ++s) o.step(); return int(TSLB_OK); })()));
 }

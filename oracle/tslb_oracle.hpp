@@ -173,6 +173,13 @@ struct Oracle {
     R& G(int q, int i, int j, int k) { return g[size_t(q) * vol + id(i, j, k)]; }
     R omega_pf() const { return R(1) / R(prm.tau_a); }
 
+    // interior solid nodes (the reference's isfluid == 0; empty: none).  Solid
+    // nodes are not stepped (moments kept, no push), their normals are 0, and
+    // populations entering fluid nodes from them are bounced back
+    // (boundary_cds_3D_module.f90:11-76 applied at every isfluid == 0 node).
+    std::vector<unsigned char> isfluid;
+    bool solid_at(int i, int j, int k) const { return !isfluid.empty() && !isfluid[iid(i, j, k)]; }
+
     // per-node correction of the colour-mode relaxation time (empty: none);
     // the B200 path's tslb_set_tau_correction and learned closure
     std::vector<R> dtau;
@@ -260,6 +267,7 @@ struct Oracle {
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
+                    if (solid_at(i, j, k)) continue;  // solid nodes keep their moments
                     size_t x = id(i, j, k);
                     R tot[27];
                     R rho_a = 0, rho_b = 0;
@@ -320,6 +328,7 @@ struct Oracle {
                     R mod = std::sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
                     R den = mod + R(1e-9);
                     size_t x = id(i, j, k);
+                    if (solid_at(i, j, k)) gr[0] = gr[1] = gr[2] = R(0);
                     nrm[0][x] = gr[0] / den;
                     nrm[1][x] = gr[1] / den;
                     nrm[2][x] = gr[2] / den;
@@ -336,6 +345,7 @@ struct Oracle {
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
+                    if (solid_at(i, j, k)) continue;
                     size_t x = id(i, j, k);
                     const R rho = M[RHO][x], u = M[UX][x], v = M[UY][x], w = M[UZ][x];
                     const R P[6] = {M[PXX][x], M[PXY][x], M[PXZ][x], M[PYY][x], M[PYZ][x], M[PZZ][x]};
@@ -399,6 +409,7 @@ struct Oracle {
         for (int k = 0; k < nz; ++k)
             for (int j = 0; j < ny; ++j)
                 for (int i = 0; i < nx; ++i) {
+                    if (solid_at(i, j, k)) continue;
                     size_t x = id(i, j, k);
                     const R rho = M[RHO][x], u = M[UX][x], v = M[UY][x], w = M[UZ][x];
                     const R P[6] = {M[PXX][x], M[PXY][x], M[PXZ][x], M[PYY][x], M[PYZ][x], M[PZZ][x]};
@@ -588,6 +599,37 @@ struct Oracle {
                             G(q, wi, wj, wk) = G(q, i, j, k);
                         }
                 }
+        // (4) half-way bounce-back at interior solid nodes, after the wrap so
+        //     that populations that crossed a periodic face have arrived:
+        //     f(x+c_i, i) = f(x, opp(i)) for fluid x+c_i (periodic axes wrap)
+        if (!isfluid.empty()) {
+            auto wrap = [&](int v, int a, bool& ok) {
+                const int n = dim(a);
+                if (v >= 0 && v < n) return v;
+                if (periodic(a)) return (v + n) % n;
+                ok = false;
+                return v;
+            };
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        if (!solid_at(i, j, k)) continue;
+                        for (int q = 1; q < 27; ++q) {
+                            bool ok = true;
+                            const int ti = wrap(i + CX[q], 0, ok), tj = wrap(j + CY[q], 1, ok), tk = wrap(k + CZ[q], 2, ok);
+                            if (!ok || solid_at(ti, tj, tk)) continue;
+                            F(q, ti, tj, tk) = F(OPP[q], i, j, k);
+                            if (colour) G(q, ti, tj, tk) = G(OPP[q], i, j, k);
+                        }
+                        if (!colour)
+                            for (int q = 1; q < 7; ++q) {
+                                bool ok = true;
+                                const int ti = wrap(i + GX[q], 0, ok), tj = wrap(j + GY[q], 1, ok), tk = wrap(k + GZ[q], 2, ok);
+                                if (!ok || solid_at(ti, tj, tk)) continue;
+                                G(q, ti, tj, tk) = G(GOPP[q], i, j, k);
+                            }
+                    }
+        }
     }
 
     // ------------------------------------------------------------------
