@@ -18,6 +18,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_STATE = range(
 MODE_PHASEFIELD, MODE_COLOUR, MODE_SINGLE = 0, 1, 2
 PREC_FP32, PREC_BF16, PREC_FP16S = 0, 1, 2
 BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET, BC_PRESSURE = range(6)
+MBC_NONE, MBC_COPY, MBC_JET = range(3)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
 NREDUCE = 12
 NOALLOC_MAX_NODES = 1 << 20
@@ -189,6 +190,10 @@ def lib() -> ctypes.CDLL:
         lp = ctypes.POINTER(ctypes.c_longlong)
         L.tslb_set_inlet_disc.argtypes = [vp, ip] + [ctypes.c_float] * 5 + [ctypes.c_ulonglong] * 2
         L.tslb_set_inlet_disc.restype = ip
+        L.tslb_set_moment_bc.argtypes = [vp, ip, ip, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        L.tslb_set_moment_bc.restype = ip
+        L.tslb_rand_noseeded.argtypes = [ip, ip, ip, ip]
+        L.tslb_rand_noseeded.restype = ctypes.c_float
         L.tslb_set_solid_mask.argtypes = [vp, vp]
         L.tslb_set_solid_mask.restype = ip
         L.tslb_set_tau_correction.argtypes = [vp, fp]

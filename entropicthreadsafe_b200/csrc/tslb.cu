@@ -284,6 +284,34 @@ __global__ void inlet_disc_kernel(float* plane, int n0, int n1, int axis, float 
     plane[3 * pa + i] = in ? 1.0f : -1.0f;
 }
 
+// moment-space boundary plane of face (4: z = 0, 5: z = nz - 1), see tslb_set_moment_bc
+template <class T>
+__global__ void moment_bc_kernel(StepArgs a, T* st, int face, int kind, float uwall, float r2, float amp, int step) {
+    const long long plane = (long long)a.nx * a.ny;
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    const int k0 = face == 4 ? 0 : a.nz - 1, k1 = face == 4 ? 1 : a.nz - 2;
+    const long long i0 = (long long)k0 * plane + p, i1 = (long long)k1 * plane + p;
+    if (kind == TSLB_MBC_COPY) {
+        for (int f = 0; f < NF; ++f) st[f * a.N + i0] = st[f * a.N + i1];
+        return;
+    }
+    // TSLB_MBC_JET: rho - 1 and Pi from the next plane, tangential velocity 0
+    st[F_D * a.N + i0] = st[F_D * a.N + i1];
+    for (int f = F_XX; f <= F_ZZ; ++f) st[f * a.N + i0] = st[f * a.N + i1];
+    st[F_U * a.N + i0] = cvt_out<T>(0.f, a, F_U);
+    st[F_V * a.N + i0] = cvt_out<T>(0.f, a, F_V);
+    if (step % 10 == 0) {
+        const int i = (int)(p % a.nx) + 1, j = (int)(p / a.nx) + 1;   // 1-based
+        const float dx = (float)i - a.nx / 2.0f, dy = (float)j - a.ny / 2.0f;
+        if (dx * dx + dy * dy <= r2) {
+            const float r = fmaxf(rand_noseeded(i, j, 1, step), 2.98023224e-8f);
+            const float w = uwall + amp * sqrtf(-2.0f * logf(r)) * cosf(6.283185307179586f * r);
+            st[F_W * a.N + i0] = cvt_out<T>(w, a, F_W);
+        }
+    }
+}
+
 // solid bit mask from isfluid bytes: word w holds nodes 32w .. 32w+31
 __global__ void solid_bits_kernel(const unsigned char* __restrict__ isfluid, long long n, unsigned int* solid) {
     const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -455,7 +483,29 @@ void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) 
     });
 }
 
+int launch_moment_bcs(tslb_ctx* c) {
+    for (int face = 4; face < 6; ++face) {
+        if (c->mbc_kind[face] == TSLB_MBC_NONE) continue;
+        StepArgs a = make_args(c, nullptr, nullptr);
+        const long long plane = (long long)c->nx * c->ny;
+        const int step = (int)((c->steps_done + 1) % 2000000000LL);
+        with_storage(c->p.precision, [&](auto tag) {
+            using T = decltype(tag);
+            moment_bc_kernel<T><<<(unsigned)((plane + 255) / 256), 256, 0, c->stream>>>(
+                a, static_cast<T*>(c->state[c->cur]), face, c->mbc_kind[face], c->mbc_uwall[face],
+                c->mbc_radius[face] * c->mbc_radius[face], c->mbc_amp[face], step);
+        });
+        c->launches++;
+        CUDA_TRY(c, cudaGetLastError());
+    }
+    return TSLB_OK;
+}
+
 int launch_step(tslb_ctx* c) {
+    {
+        int rc = launch_moment_bcs(c);
+        if (rc) return rc;
+    }
     if (c->p.mode == TSLB_MODE_PHASEFIELD) {
         int rc = launch_normals(c);
         if (rc) return rc;
@@ -811,6 +861,22 @@ int tslb_set_inlet_disc(tslb_ctx* c, int face, float c0, float c1, float radius,
                                                                           radius * radius, speed, amp, seed, counter);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
+float tslb_rand_noseeded(int i, int j, int k, int l) { return rand_noseeded(i, j, k, l); }
+
+int tslb_set_moment_bc(tslb_ctx* c, int face, int kind, float uwall, float radius, float amp) {
+    if (!c) return TSLB_ERR_ARG;
+    if (face != 4 && face != 5) return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_moment_bc: z faces (4, 5) only");
+    if (kind < TSLB_MBC_NONE || kind > TSLB_MBC_JET) return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: unknown kind");
+    if (c->nz < 3) return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: nz must be >= 3");
+    if (!std::isfinite(uwall) || !std::isfinite(radius) || !std::isfinite(amp))
+        return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: non-finite argument");
+    c->mbc_kind[face] = kind;
+    c->mbc_uwall[face] = uwall;
+    c->mbc_radius[face] = radius;
+    c->mbc_amp[face] = amp;
     return TSLB_OK;
 }
 

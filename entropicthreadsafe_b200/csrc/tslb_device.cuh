@@ -85,6 +85,38 @@ struct StepArgs {
     const unsigned int* near;   // fluid nodes with a solid one among their 26 neighbours, same layout
 };
 
+// Counter-based uniform in [0, 1) of four integers: the reference's
+// rand_noseeded (TSLB_2C-mpi/vars_single_3D_module.f90:150-215), which seeds
+// the two lagged generators of the Marsaglia-Zaman "universal" method from
+// (i, j, k, l) in 24 rounds each and returns one output.  Every FP32 value
+// is a multiple of 2^-24 in [-1, 2), so the arithmetic is exact and equal
+// on the host, on the device and in the Fortran original.
+__host__ __device__ inline float rand_noseeded(int i, int j, int k, int l) {
+    int isub = i % 178 + 1, jsub = j % 178 + 1, ksub = k % 178 + 1, lsub = l % 169;
+    float u[2];
+    for (int g = 0; g < 2; ++g) {
+        float s = 0.f, t = 0.5f;
+        for (int jj = 0; jj < 24; ++jj) {
+            const int msub = ((isub * jsub) % 179) * ksub % 179;
+            isub = jsub;
+            jsub = ksub;
+            ksub = msub;
+            lsub = (53 * lsub + 1) % 169;
+            if ((lsub * msub) % 64 >= 32) s += t;
+            t *= 0.5f;
+        }
+        u[g] = s;   // u97, then u33
+    }
+    float uni = u[0] - u[1];
+    if (uni < 0.f) uni += 1.f;
+    const float c = 362436.0f / 16777216.0f, cd = 7654321.0f / 16777216.0f, cm = 16777213.0f / 16777216.0f;
+    float csub = c - cd;
+    if (csub < 0.f) csub += cm;
+    uni -= csub;
+    if (uni < 0.f) uni += 1.f;
+    return uni;
+}
+
 __device__ __forceinline__ bool bit_at(const unsigned int* b, long long i) {
     return (__ldg(b + (i >> 5)) >> (i & 31)) & 1u;
 }

@@ -42,6 +42,9 @@ struct tslb_ctx {
     unsigned int* solid = nullptr;
     unsigned int* near = nullptr;
     bool solid_on = false;
+    // moment-space boundary planes (tslb_set_moment_bc), per face
+    int mbc_kind[6] = {0, 0, 0, 0, 0, 0};
+    float mbc_uwall[6], mbc_radius[6], mbc_amp[6];
     tslb_closure* closure = nullptr;       // attached closure (not owned)
     int closure_interval = 1;
     long long steps_done = 0;

@@ -87,6 +87,10 @@ class Lattice:
         """Jet inlet drawn on the device (see tslb_set_inlet_disc; workloads.inlet_disc is its host mirror)."""
         self._check(self.L.tslb_set_inlet_disc(self.h, face, c0, c1, radius, speed, amp, int(seed), int(counter)))
 
+    def set_moment_bc(self, face: int, kind: int, uwall: float = 0.0, radius: float = 10.0, amp: float = 0.004) -> None:
+        """Moment-space boundary plane of a z face (tslb_set_moment_bc)."""
+        self._check(self.L.tslb_set_moment_bc(self.h, face, kind, uwall, radius, amp))
+
     def set_solid_mask(self, isfluid) -> None:
         """Interior solid nodes: isfluid (nz, ny, nx), 1 fluid / 0 solid, or None."""
         if isfluid is None:

@@ -176,6 +176,27 @@ int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
  * four planes (u, v, w, phi) of the face's extent, Fortran order. */
 int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
 
+/* ---- moment-space boundary planes (TSLB_newBCS/boundary_cds_3D_module.f90:1233-1292) ----
+ * Before every step the moments of the face plane (z faces: z = 0 or nz-1)
+ * are rewritten from the plane next to it, between the moments pass and the
+ * collision as bcs_TSLB_only_z_turbojet does:
+ *   TSLB_MBC_COPY  all moments copied from the next plane inward (its k = nz side)
+ *   TSLB_MBC_JET   rho and Pi copied from the next plane, u = v = 0; w keeps the
+ *                  stepped value, except on every 10th step (reference step
+ *                  numbering, step = steps done + 1) when the nodes of the disc
+ *                  (i - nx/2)^2 + (j - ny/2)^2 <= radius^2 (1-based i, j) get
+ *                  w = uwall + amp sqrt(-2 ln r) cos(2 pi r), r = rand_noseeded(i, j, 1, step)
+ *                  (its k = 1 side; r is floored at 2^-25 so w stays finite)
+ * The populations that enter the plane from outside follow the face's kind
+ * as usual (the reference leaves its z halo untouched). */
+#define TSLB_MBC_NONE  0
+#define TSLB_MBC_COPY  1
+#define TSLB_MBC_JET   2
+int  tslb_set_moment_bc(tslb_ctx* ctx, int face, int kind, float uwall, float radius, float amp);
+/* The reference's counter-based uniform rand_noseeded(i, j, k, l)
+ * (TSLB_2C-mpi/vars_single_3D_module.f90:150-215), bit-exact. */
+float tslb_rand_noseeded(int i, int j, int k, int l);
+
 /* Interior solid nodes: isfluid holds nx*ny*nz bytes (Fortran order), 1 for
  * a fluid node and 0 for a solid one, as the reference's isfluid array
  * (recursive_2c_TSLB3D.f90:79-85); NULL removes them.  Populations that
