@@ -61,6 +61,34 @@ struct Src {
     }
 };
 
+// The mirror sources of cx = +1 and cx = -1 (same cy) evaluated together as
+// one float2 on the paired FP32 instructions of sm_100 (x: cx = +1, y: cx = -1);
+// the factors +-1 are exact, so each lane is the scalar evaluation.
+template <int CYv>
+struct SrcPair {
+    const float* Ka;   // source of cx = +1
+    const float* Kb;   // source of cx = -1
+    __device__ __forceinline__ float2 L(int slot) const { return make_float2(Ka[slot * CAREA], Kb[slot * CAREA]); }
+    __device__ __forceinline__ void eval(float2& Pm, float2& P0, float2& Pp) const {
+        const float2 sx = make_float2(1.f, -1.f);
+        float2 q0 = __fadd2_rn(L(K_0), __ffma2_rn(sx, L(K_X), L(K_XX)));
+        float2 q1 = __fadd2_rn(L(K_Z), __ffma2_rn(sx, L(K_XZ), L(K_XXZ)));
+        float2 q2 = __ffma2_rn(sx, L(K_XZZ), L(K_ZZ));
+        if (CYv) {
+            const float2 cy = make_float2((float)CYv, (float)CYv), sxy = make_float2((float)CYv, (float)-CYv);
+            q0 = __fadd2_rn(q0, __ffma2_rn(cy, L(K_Y), L(K_YY)));
+            q0 = __fadd2_rn(q0, __ffma2_rn(sxy, L(K_XY), __ffma2_rn(cy, L(K_XXY), __fmul2_rn(sx, L(K_XYY)))));
+            q1 = __fadd2_rn(q1, __ffma2_rn(cy, L(K_YZ), L(K_YYZ)));
+            q1 = __ffma2_rn(sxy, L(K_XYZ), q1);
+            q2 = __ffma2_rn(cy, L(K_YZZ), q2);
+        }
+        const float2 t = __fadd2_rn(q0, q2);
+        Pm = __ffma2_rn(make_float2(-1.f, -1.f), q1, t);
+        P0 = q0;
+        Pp = __fadd2_rn(t, q1);
+    }
+};
+
 __host__ __device__ constexpr float w1d(int c) { return c == 0 ? 2.0f / 3.0f : 1.0f / 6.0f; }
 
 // Moments of the three populations of one (cy, cz) group: directions
@@ -111,9 +139,12 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
     const Src<0, CYv> sz{Kc - CYv * CW};       // source of cx = 0
     const Src<-1, CYv> sb{Kc - CYv * CW + 1};  // source of cx = -1 (x + 1)
     float am, a0, ap, cm, c0, cp, bm, b0, bp;
-    sa.eval(am, a0, ap);
+    {
+        float2 pm, p0, pp;
+        SrcPair<CYv>{sa.Kp, sb.Kp}.eval(pm, p0, pp);
+        am = pm.x; bm = pm.y; a0 = p0.x; b0 = p0.y; ap = pp.x; bp = pp.y;
+    }
     sz.eval(cm, c0, cp);
-    sb.eval(bm, b0, bp);
     acc_group<CYv, -1>(accm, am, cm, bm);
     acc_group<CYv, 0>(acc0, a0, c0, b0);
     acc_group<CYv, 1>(accp, ap, cp, bp);
