@@ -173,7 +173,8 @@ struct ArraySrc {
         }
         return ok;
     }
-    __device__ void store(long long i, float y) const { out[i] = y; }
+    __device__ float keep(const Raw&) const { return 0.f; }
+    __device__ void store(long long i, float y, float) const { out[i] = y; }
 };
 
 // features of lattice node i from the FP32 moment state; dtau is read (the
@@ -186,8 +187,9 @@ struct LatticeSrc {
     float inv_nu_a, inv_nu_b;
     float* dtau;         // total correction of the previous refresh, rewritten (null: none)
     const float* base;   // static correction (tslb_set_tau_correction) or null
+    Divider dx, dy;      // division by nx, ny
     struct Raw {
-        float P[6], phi, u, v, w, ph[6], dprev;
+        float P[6], phi, u, v, w, ph[6], dprev, dbase;
     };
     __device__ float phi_at(int x, int y, int z) const {
         return st[F_PHI * N + x + (long long)nx * (y + (long long)ny * z)];
@@ -196,9 +198,9 @@ struct LatticeSrc {
         if (i >= n) return;
         int x, y, z;
         if (n < (1LL << 31)) {
-            const int ii = (int)i, q = ii / nx;
+            const int ii = (int)i, q = dx.div(ii);
             x = ii - q * nx;
-            z = q / ny;
+            z = dy.div(q);
             y = q - z * ny;
         } else {
             x = (int)(i % nx); y = (int)((i / nx) % ny); z = (int)(i / ((long long)nx * ny));
@@ -214,20 +216,23 @@ struct LatticeSrc {
         r.ph[4] = phi_at(x, y, nbr(z, 1, nz, pz));
         r.ph[5] = phi_at(x, y, nbr(z, -1, nz, pz));
         r.dprev = dtau ? dtau[i] : 0.f;
+        r.dbase = base ? base[i] : 0.f;
     }
     __device__ bool features(const Raw& r, long long, float* f) const {
         const float gx = 0.5f * (r.ph[0] - r.ph[1]), gy = 0.5f * (r.ph[2] - r.ph[3]), gz = 0.5f * (r.ph[4] - r.ph[5]);
-        // plain tau of the node's mixture: 1/omega = (6 + q)/(2q)
+        // plain tau of the node's mixture: 1/omega = (6 + q)/(2q), and
+        // s = tau / (tau + dprev) = (6 + q) / (6 + q + 2 q dprev)
         const float q = 0.5f * ((inv_nu_a + inv_nu_b) + r.phi * (inv_nu_a - inv_nu_b));
-        const float tau = (6.f + q) / (2.f * q);
-        const float s = tau / (tau + r.dprev);
+        const float s = (6.f + q) / fmaf(2.f * q, r.dprev, 6.f + q);
         make_features(s, r.P, r.phi, sqrtf(gx * gx + gy * gy + gz * gz), sqrtf(r.u * r.u + r.v * r.v + r.w * r.w), f);
         bool ok = true;
 #pragma unroll
         for (int k = 0; k < NFEAT; ++k) ok = ok && isfinite(f[k]);
         return ok;
     }
-    __device__ void store(long long i, float y) const { dtau[i] = base ? y + base[i] : y; }
+    // the static correction, read with the inputs so the store waits on nothing
+    __device__ float keep(const Raw& r) const { return r.dbase; }
+    __device__ void store(long long i, float y, float b) const { dtau[i] = y + b; }
 };
 
 // Inference: dtau = dtau_max sigmoid(o) for every row of the source, 128
@@ -252,6 +257,7 @@ __global__ void __launch_bounds__(TILE, 6) infer_kernel(const Image* __restrict_
         const bool valid = i < n;
         float f[NFEAT];
         const bool fin = valid && src.features(raw, i, f);
+        const float kept = src.keep(raw);
         if (t + gridDim.x < ntiles) src.load((t + gridDim.x) * TILE + tid, raw);
         put_x<NCH_INFER>(S.act, tid, f, im, fin);
         sync_for_mma();
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(TILE, 6) infer_kernel(const Image* __restrict_
         // stability clamp: the plain tau where anything is not finite
         if (!fin || !isfinite(y)) y = 0.f;
         y = fminf(fmaxf(y, 0.f), im.dtau_max);
-        if (valid) src.store(i, y);
+        if (valid) src.store(i, y, kept);
     }
     smem_teardown(S, tb, 64, ph);
 }
@@ -709,6 +715,8 @@ LatticeSrc lattice_src(tslb_ctx* L, const float* view) {
     s.inv_nu_b = 3.0f / (L->p.tau_b - 0.5f);
     s.dtau = L->dtau;
     s.base = L->base_on ? L->dtau_base : nullptr;
+    s.dx = Divider::make(L->nx);
+    s.dy = Divider::make(L->ny);
     return s;
 }
 

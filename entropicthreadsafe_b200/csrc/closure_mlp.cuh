@@ -70,6 +70,16 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 __device__ __forceinline__ uint4 pack8(const float* v) {
     return make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
 }
+// bf16(max(a, 0)) | bf16(max(b, 0)) << 16 in one conversion (a in the low half,
+// as pack2); for finite inputs equal to pack2(fmaxf(a, 0), fmaxf(b, 0))
+__device__ __forceinline__ uint32_t pack2_relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
+__device__ __forceinline__ uint4 pack8_relu(const float* v) {
+    return make_uint4(pack2_relu(v[0], v[1]), pack2_relu(v[2], v[3]), pack2_relu(v[4], v[5]), pack2_relu(v[6], v[7]));
+}
 
 // ---- MMA issue (one thread) ----
 template <int NCH = NCH_TRAIN>
@@ -159,24 +169,31 @@ __device__ __forceinline__ uint64_t epi_h1(uint32_t tb, uint4* act, int s, uint3
             mask |= (uint64_t)m << (32 * q);
         }
 #pragma unroll
-        for (int j = 0; j < 32; ++j) z[j] = fmaxf(z[j], 0.f);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) act[Act<NCH>::chunk(s, 4 * q + c)] = pack8(z + 8 * c);
+        for (int c = 0; c < 4; ++c) act[Act<NCH>::chunk(s, 4 * q + c)] = pack8_relu(z + 8 * c);
     }
     return mask;
 }
 
-// network output o = w3 . relu(z2 + b2) + b3 (four partial sums)
+// network output o = w3 . relu(z2 + b2) + b3 in four partial sums (units
+// j = 0, 1, 2, 3 mod 4), the bias add and the products on the paired FP32
+// instructions
 __device__ __forceinline__ float epi_out(uint32_t tb, const Image& im, uint32_t col = COL_Z2) {
-    float o[4] = {im.b3, 0.f, 0.f, 0.f};
+    float2 o[2] = {make_float2(im.b3, 0.f), make_float2(0.f, 0.f)};
+    const float2* b2 = reinterpret_cast<const float2*>(im.b2);
+    const float2* w3 = reinterpret_cast<const float2*>(im.w3);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         float z[32];
         tc::tmem_ld32(lane_addr(tb, col + 32 * q), z);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) o[j & 3] = fmaf(im.w3[32 * q + j], fmaxf(z[j] + im.b2[32 * q + j], 0.f), o[j & 3]);
+        for (int j = 0; j < 32; j += 2) {
+            float2 v = __fadd2_rn(make_float2(z[j], z[j + 1]), b2[(32 * q + j) >> 1]);
+            v.x = fmaxf(v.x, 0.f);
+            v.y = fmaxf(v.y, 0.f);
+            o[(j >> 1) & 1] = __ffma2_rn(w3[(32 * q + j) >> 1], v, o[(j >> 1) & 1]);
+        }
     }
-    return (o[0] + o[1]) + (o[2] + o[3]);
+    return (o[0].x + o[0].y) + (o[1].x + o[1].y);
 }
 
 // dz2 = g w3 [z2 + b2 > 0] into DZ chunks 0..7; dw3 += g h2
@@ -224,6 +241,27 @@ __device__ __forceinline__ void make_features(float s, const float* P, float phi
     f[8] = umag;
     f[9] = s * frob(P);
 }
+// Division by an invariant divisor d >= 1 of dividends 0 <= n < 2^31 with a
+// multiply-high and a shift (the round-up method of Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994): with
+// l = ceil(log2 d) and m = ceil(2^(31+l) / d) < 2^32, the error of m / 2^(31+l)
+// against 1/d is below 1/(d n) for every n < 2^31, so
+// n / d = floor(n m / 2^(31+l)) = umulhi(n, m) >> (l - 1).  d = 1 keeps m = 0.
+struct Divider {
+    uint32_t m = 0;
+    int sh = 0;
+    static Divider make(int d) {
+        Divider r;
+        if (d <= 1) return r;
+        int l = 0;
+        while ((1LL << l) < d) ++l;
+        r.m = (uint32_t)((((unsigned long long)1 << (31 + l)) + (unsigned long long)d - 1) / (unsigned long long)d);
+        r.sh = l - 1;
+        return r;
+    }
+    __device__ __forceinline__ int div(int n) const { return m ? (int)(__umulhi((uint32_t)n, m) >> sh) : n; }
+};
+
 // neighbour coordinate: periodic axes wrap, others repeat the boundary node
 __device__ __forceinline__ int nbr(int x, int d, int n, bool periodic) {
     int y = x + d;
