@@ -215,11 +215,16 @@ __global__ void pops_to_moments_kernel(int nx, int ny, int nz, long long N, int 
 }
 
 // FP64 diagnostics: sums in TSLB_RED_* order (8..9 hold sums of rho and
-// counts inside/outside; finalised on the host), umax as float bits.
-constexpr int RED_SLOTS = 12;
-__global__ void reduce_kernel(const float* __restrict__ s, long long n, long long N, int colour, double* red) {
-    __shared__ double sh[RED_SLOTS][8];
-    __shared__ float shmax[8];
+// counts inside/outside; finalised on the host) and, in part RED_SLOTS, the
+// maximum of |u|^2.  Every block writes its partials; the last block to
+// finish (ticket) adds them up in block order, so the result depends only on
+// the state and the grid, never on the order in which blocks finish.
+constexpr int RED_SLOTS = 12, RED_PARTS = RED_SLOTS + 1, RED_THREADS = 256;
+__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const float* __restrict__ s, long long n, long long N,
+                                                             int colour, double* part, double* out,
+                                                             unsigned int* ticket) {
+    __shared__ double sh[RED_PARTS][RED_THREADS / 32];
+    __shared__ bool last;
     double acc[RED_SLOTS];
     for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
     float umax2 = 0.f;
@@ -238,24 +243,49 @@ __global__ void reduce_kernel(const float* __restrict__ s, long long n, long lon
         if (phi < lo) { acc[9] += rho; acc[10] += 1.0; }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < RED_SLOTS; ++k) {
-        double vv = acc[k];
-        for (int o = 16; o > 0; o >>= 1) vv += __shfl_down_sync(0xffffffffu, vv, o);
+    // block partials: a fixed shuffle tree per warp, then the warps in order
+    for (int k = 0; k < RED_PARTS; ++k) {
+        double vv = k < RED_SLOTS ? acc[k] : (double)umax2;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, vv, o);
+            vv = k < RED_SLOTS ? vv + t : fmax(vv, t);
+        }
         if (lane == 0) sh[k][warp] = vv;
     }
-    for (int o = 16; o > 0; o >>= 1) umax2 = fmaxf(umax2, __shfl_down_sync(0xffffffffu, umax2, o));
-    if (lane == 0) shmax[warp] = umax2;
     __syncthreads();
-    if (threadIdx.x < RED_SLOTS) {
-        double t = 0.0;
-        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) t += sh[threadIdx.x][w8];
-        atomicAdd(&red[threadIdx.x], t);
+    if (threadIdx.x < RED_PARTS) {
+        const int k = threadIdx.x;
+        double t = sh[k][0];
+        for (int w8 = 1; w8 < RED_THREADS / 32; ++w8) t = k < RED_SLOTS ? t + sh[k][w8] : fmax(t, sh[k][w8]);
+        part[(long long)blockIdx.x * RED_PARTS + k] = t;
     }
-    if (threadIdx.x == 0) {
-        float m = 0.f;
-        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) m = fmaxf(m, shmax[w8]);
-        atomicMax(reinterpret_cast<unsigned int*>(&red[RED_SLOTS]), __float_as_uint(m));
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last block: thread t takes blocks t, t + 256, ... in order, then the same trees
+    for (int k = 0; k < RED_PARTS; ++k) {
+        double vv = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += RED_THREADS) {
+            const double p = __ldcg(part + (long long)b * RED_PARTS + k);
+            vv = k < RED_SLOTS ? vv + p : fmax(vv, p);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, vv, o);
+            vv = k < RED_SLOTS ? vv + t : fmax(vv, t);
+        }
+        if (lane == 0) sh[k][warp] = vv;
     }
+    __syncthreads();
+    if (threadIdx.x < RED_PARTS) {
+        const int k = threadIdx.x;
+        double t = sh[k][0];
+        for (int w8 = 1; w8 < RED_THREADS / 32; ++w8) t = k < RED_SLOTS ? t + sh[k][w8] : fmax(t, sh[k][w8]);
+        out[k] = t;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // splitmix64 finaliser (Steele, Lea, Flood 2014)
@@ -646,7 +676,16 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->io, sizeof(float) * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(io)");
     if ((e = cudaMalloc(&c->nrm, sizeof(float) * 3 * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(normals)");
     if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
-    if ((e = cudaMalloc(&c->red, sizeof(double) * (RED_SLOTS + 1))) != cudaSuccess) return bail(e, "cudaMalloc(reduce)");
+    {
+        int sm_count = 148;
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c->device);
+        c->red_blocks = 4 * sm_count;
+        // partials, results, ticket (one more double)
+        const size_t red_bytes = sizeof(double) * ((size_t)c->red_blocks * RED_PARTS + RED_PARTS + 1);
+        if ((e = cudaMalloc(&c->red, red_bytes)) != cudaSuccess) return bail(e, "cudaMalloc(reduce)");
+        if ((e = cudaMemset(c->red, 0, red_bytes)) != cudaSuccess) return bail(e, "cudaMemset(reduce)");
+        if ((e = cudaMallocHost(&c->red_host, sizeof(double) * RED_PARTS)) != cudaSuccess) return bail(e, "cudaMallocHost(reduce)");
+    }
     if ((e = cudaMemset(c->flags, 0, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMemset");
     for (int f = 0; f < 6; ++f) {
         if (p->bc[f] != TSLB_BC_INLET) continue;
@@ -674,6 +713,7 @@ void tslb_destroy(tslb_ctx* c) {
     cudaFree(c->nrm);
     cudaFree(c->flags);
     cudaFree(c->red);
+    cudaFreeHost(c->red_host);
     cudaFree(c->dtau);
     cudaFree(c->dtau_base);
     cudaFree(c->solid);
@@ -807,22 +847,19 @@ int tslb_download_normals(tslb_ctx* c, float* nx, float* ny, float* nz) {
 int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
     if (!c || !out) return fail(c, TSLB_ERR_ARG, "tslb_reduce: NULL");
     if (!c->loaded) return fail(c, TSLB_ERR_STATE, "reduce before an upload");
-    CUDA_TRY(c, cudaMemsetAsync(c->red, 0, sizeof(double) * (RED_SLOTS + 1), c->stream));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const float* view = nullptr;
     int rc = fp32_view(c, &view);
     if (rc) return rc;
-    reduce_kernel<<<(unsigned)(sms * 4), 256, 0, c->stream>>>(view, c->n, c->N, c->p.mode == TSLB_MODE_COLOUR, c->red);
+    double* results = c->red + (size_t)c->red_blocks * RED_PARTS;
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(results + RED_PARTS);
+    reduce_kernel<<<(unsigned)c->red_blocks, RED_THREADS, 0, c->stream>>>(view, c->n, c->N, c->p.mode == TSLB_MODE_COLOUR,
+                                                                          c->red, results, ticket);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
-    double h[RED_SLOTS + 1];
-    CUDA_TRY(c, cudaMemcpyAsync(h, c->red, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->red_host, results, sizeof(double) * RED_PARTS, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    unsigned int umax_bits;
-    std::memcpy(&umax_bits, &h[RED_SLOTS], sizeof(umax_bits));
-    float umax2;
-    std::memcpy(&umax2, &umax_bits, sizeof(umax2));
+    const double* h = c->red_host;
+    const double umax2 = h[RED_SLOTS];
     out[TSLB_RED_MASS] = (double)c->n + h[0];
     out[TSLB_RED_MASS_A] = h[1];
     out[TSLB_RED_MASS_B] = h[2];
@@ -830,7 +867,7 @@ int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
     out[TSLB_RED_MOM_Y] = h[4];
     out[TSLB_RED_MOM_Z] = h[5];
     out[TSLB_RED_KINETIC] = h[6];
-    out[TSLB_RED_UMAX] = std::sqrt((double)umax2);
+    out[TSLB_RED_UMAX] = std::sqrt(umax2);
     out[TSLB_RED_RHO_IN] = h[8] > 0 ? h[7] / h[8] : 0.0;
     out[TSLB_RED_RHO_OUT] = h[10] > 0 ? h[9] / h[10] : 0.0;
     out[TSLB_RED_DP] = (h[8] > 0 && h[10] > 0) ? (out[TSLB_RED_RHO_IN] - out[TSLB_RED_RHO_OUT]) / 3.0 : 0.0;

@@ -26,7 +26,11 @@ struct tslb_ctx {
     float* nrm = nullptr;                  // 3 fields
     float* inlet[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     unsigned int* flags = nullptr;
-    double* red = nullptr;                 // reduction accumulators
+    // FP64 diagnostics: red_blocks x RED_PARTS per-block partials, then the
+    // RED_PARTS results and the last-block ticket; red_host is pinned
+    double* red = nullptr;
+    double* red_host = nullptr;
+    int red_blocks = 0;
     bool loaded = false;
     int zchunk = 32;
     long long launches = 0;

@@ -335,8 +335,10 @@ struct Geo {
     static constexpr int MROWS = CH;                  // moment rows: y0-1 .. y0+TY
     static constexpr int PROWS = TY + 4;              // phi rows: y0-2 .. y0+TY+1
     static constexpr int MAREA = MROWS * SW, PAREA = PROWS * SW;
-    static constexpr int MCOPIES = NMOM * MROWS * NCH;
-    static constexpr int MROUNDS = (MCOPIES + NTHR - 1) / NTHR;
+    static constexpr int MCELLS = MROWS * NCH;        // 16-byte cells of one staged moment plane
+    static constexpr int MGROUPS = NTHR / MCELLS;     // thread (g, cell) copies fields g, g + MGROUPS, ...
+    static constexpr int MFIELDS = (NMOM + MGROUPS - 1) / MGROUPS;
+    static_assert(MGROUPS >= 1, "a staged moment plane has more cells than the block has threads");
     static constexpr int PCOPIES = PROWS * NCH;
     static constexpr int PELEMS = PROWS * SW;
     static constexpr int PEROUNDS = (PELEMS + NTHR - 1) / NTHR;
@@ -470,13 +472,14 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     // VEC: copy j < PCOPIES is the 16-byte chunk (row j / NCH, chunk j % NCH);
     // a chunk is either fully inside the domain (after the periodic wrap) or
     // fully behind a non-periodic face, whose ghost values are computed.
-    int pch_off = 0;
+    int pch_off = 0, pch_dst = 0;
     bool pch_out = true;
     if (VEC && tid < G::PCOPIES) {
         const int row = tid / G::NCH, ch = tid % G::NCH;
         const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 2 + row, xper, yper);
         pch_off = nd.off;
         pch_out = nd.out;
+        pch_dst = row * SW + EPC * ch;
     }
     auto ghost = [&](float v) { return cvt_out<T>(v, a, F_PHI); };
     auto stage_phi = [&](int z) {
@@ -486,11 +489,11 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         const T* ph = gin + F_PHI * a.N + (long long)gz * plane;
         if (VEC) {
             if (tid < G::PCOPIES) {
-                const int row = tid / G::NCH, ch = tid % G::NCH;
-                T* dst = slot + row * SW + EPC * ch;
+                T* dst = slot + pch_dst;
                 if (!pch_out && !zout) {
                     cp_async16(reinterpret_cast<float*>(dst), reinterpret_cast<const float*>(ph + pch_off));
                 } else {
+                    const int row = tid / G::NCH, ch = tid % G::NCH;
 #pragma unroll
                     for (int e = 0; e < EPC; ++e) dst[e] = ghost(phi_at<T>(a, x0 - EPC + EPC * ch + e, y0 - 2 + row, z));
                 }
@@ -514,18 +517,18 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     };
 
     // ---- staging of the 10 non-phi moments of plane z ----
-    // VEC: copy j = tid + r NTHR < MCOPIES is (field j / (MROWS NCH), row, chunk)
-    int mch_off[G::MROUNDS];
-    unsigned mch_ok = 0;
-    if (VEC) {
-#pragma unroll
-        for (int r = 0; r < G::MROUNDS; ++r) {
-            const int j = tid + r * NTHR;
-            const int rem = j % (G::MROWS * G::NCH), row = rem / G::NCH, ch = rem % G::NCH;
-            const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 1 + row, xper, yper);
-            mch_off[r] = nd.off;
-            if (j < G::MCOPIES && !nd.out) mch_ok |= 1u << r;
-        }
+    // VEC: thread tid < MGROUPS MCELLS owns cell tid % MCELLS (row, chunk) of the
+    // staged plane and copies it for the fields tid / MCELLS + k MGROUPS; the
+    // addresses are fixed per thread, only the plane changes.
+    int mcell_dst = 0, mcell_off = 0, mfg = 0;
+    bool mcell_ok = false;
+    if (VEC && tid < G::MGROUPS * G::MCELLS) {
+        const int cell = tid % G::MCELLS, row = cell / G::NCH, ch = cell % G::NCH;
+        mfg = tid / G::MCELLS;
+        const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 1 + row, xper, yper);
+        mcell_off = nd.off;
+        mcell_ok = !nd.out;
+        mcell_dst = mfg * MAREA + row * SW + EPC * ch;
     }
     auto stage_mom = [&](int z) {
         bool zout;
@@ -534,14 +537,15 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         T* dst = mst + (z & 1) * (NMOM * MAREA);
         const T* src = gin + (long long)gz * plane;
         if (VEC) {
+            if (mcell_ok) {
+                T* d = dst + mcell_dst;
+                const T* g = src + mfg * a.N + mcell_off;
 #pragma unroll
-            for (int r = 0; r < G::MROUNDS; ++r) {
-                if (!(mch_ok & (1u << r))) continue;
-                const int j = tid + r * NTHR;
-                const int f = j / (G::MROWS * G::NCH), rem = j % (G::MROWS * G::NCH);
-                const int row = rem / G::NCH, ch = rem % G::NCH;
-                cp_async16(reinterpret_cast<float*>(dst + f * MAREA + row * SW + EPC * ch),
-                           reinterpret_cast<const float*>(src + f * a.N + mch_off[r]));
+                for (int k = 0; k < G::MFIELDS; ++k) {
+                    if (G::MGROUPS * G::MFIELDS == NMOM || mfg + k * G::MGROUPS < NMOM)
+                        cp_async16(reinterpret_cast<float*>(d + k * G::MGROUPS * MAREA),
+                                   reinterpret_cast<const float*>(g + k * G::MGROUPS * a.N));
+                }
             }
         } else {
             for (int r = 0; r < nnodes; ++r) {

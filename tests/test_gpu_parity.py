@@ -197,6 +197,26 @@ def test_reduce_is_exact_and_matches_oracle():
             assert abs(rg[name] - ro[k]) <= 1e-2 * abs(ro[k]) + 1e-12, name
 
 
+def test_reduce_is_deterministic():
+    """The FP64 diagnostics add the per-block partials in block order: the
+    same state gives bit-equal results on every call, also on a lattice large
+    enough that every block of the reduction holds nodes."""
+    from entropicthreadsafe_b200.solver import Lattice
+    p, f = workloads.channel(nz=64, ndrops=10)
+    nz, ny, nx = f["rho"].shape
+    with Lattice(p, nx, ny, nz) as lat:
+        lat.upload_moments(f)
+        lat.step(3)
+        runs = [lat.reduce() for _ in range(5)]
+        st = lat.download()
+    for r in runs[1:]:
+        assert r == runs[0]
+    rho = st["rho"].astype(np.float64)
+    u2 = (st["u"].astype(np.float64) ** 2 + st["v"].astype(np.float64) ** 2 + st["w"].astype(np.float64) ** 2)
+    assert abs(runs[0]["mass"] - rho.sum()) <= 1e-7 * rho.size
+    assert abs(runs[0]["umax"] - np.sqrt(u2.max())) <= 1e-6 * np.sqrt(u2.max())
+
+
 def test_uniform_colour_is_kept_exactly():
     """A single-colour flow (phi = -1 everywhere) keeps phi bit-exactly: the
     colour update is an increment that vanishes where phi is uniform."""
