@@ -143,24 +143,25 @@ class ClockSampler:
 
 def cpu_baseline(max_seconds: float = 20.0):
     """Time the oracle (C++ restatement of the reference CPU path, OpenMP, FP32)
-    on the channel workload: full size if a step fits the budget, else z-slab samples."""
+    on the channel workload: full size if a step fits the budget, else slabs of
+    fewer x columns (the full wall-to-wall depth, droplets in proportion)."""
     import oracle
     from entropicthreadsafe_b200 import workloads
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    nz = 128
+    nx = 384
     while True:
-        p, f = workloads.channel(nz=nz) if nz == 128 else workloads.channel(nz=nz, ndrops=max(1, 40 * nz // 128))
-        ny, nx = f["rho"].shape[1], f["rho"].shape[2]
+        p, f = workloads.channel() if nx == 384 else workloads.channel(nx=nx, ndrops=max(1, 40 * nx // 384))
+        nz, ny = f["rho"].shape[0], f["rho"].shape[1]
         o = oracle.Oracle(p, nx, ny, nz, fp64=False, fast=True)
         o.set_moments({k: v.astype(np.float64) for k, v in f.items()})
         t0 = time.perf_counter()
         o.step(1)
         t1 = time.perf_counter() - t0
-        if t1 * 3 <= max_seconds or nz <= 8:
+        if t1 * 3 <= max_seconds or nx <= 24:
             break
         o.close()
-        nz = max(8, nz // 2)
+        nx = max(24, nx // 2)
     steps = max(1, int(max_seconds / max(t1, 1e-6)) - 1)
     steps = min(steps, 50)
     t0 = time.perf_counter()
@@ -209,14 +210,20 @@ def e2e_run(args, p, f, ws):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     lat2 = Lattice(p, nx, ny, nz)
+    t1 = time.perf_counter()
     lat2.upload_moments(host_in)
+    t2 = time.perf_counter()
     for _ in range(args.steps):
         lat2.step(1)
         lat2.reduce()
+    t3 = time.perf_counter()
     lat2.download(host_out)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    t4 = time.perf_counter()
+    e2e_s = t4 - t0
     lat2.close()
+    parts = {"create_ms": (t1 - t0) * 1e3, "upload_ms": (t2 - t1) * 1e3,
+             "step_and_reduce_ms_per_step": (t3 - t2) * 1e3 / args.steps, "download_ms": (t4 - t3) * 1e3}
     if ws > 1:
         import torch.distributed as dist
         t = torch.tensor([e2e_s], device="cuda")
@@ -227,7 +234,7 @@ def e2e_run(args, p, f, ws):
             "h2d_bytes_per_step": state_bytes / args.steps,
             "d2h_bytes_per_step": state_bytes / args.steps + 8 * capi.NREDUCE,
             "what": "tslb_create + tslb_upload_moments (pinned host) + K x (tslb_step(1) + tslb_reduce) "
-                    "+ tslb_download_moments, wall clock, per step"}
+                    "+ tslb_download_moments, wall clock, per step", "parts": parts}
 
 
 def ensemble_leg(args, ndomains: int = 48):
@@ -416,11 +423,15 @@ def run_ours(args):
     ms_max = max_over_ranks(ms)
     value = whole_job_mlups(ws, nodes, args.steps, ms_max)
     ms_step = ms_max / args.steps
+    lat.close()
+    # ---- end to end through the public API with host buffers (the same workload,
+    # right after the device-resident run: its lattice reuses that run's memory) ----
+    barrier_sync()
+    e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     # ---- precision forms of the same workload (bf16, fp16 with per-field scale) ----
     forms = None
     if not args.no_precision_forms:
         forms = {}
-        lat.close()
         for name, prec in (("bf16", capi.PREC_BF16), ("fp16s", capi.PREC_FP16S)):
             p.precision = prec
             lp = Lattice(p, nx, ny, nz)
@@ -439,15 +450,10 @@ def run_ours(args):
                            "speedup_vs_fp32": ms_step / ms_p, "bytes_per_lu": 44}
             lp.close()
         p.precision = capi.PREC_FP32
-        lat = None
-    # ---- end to end through the public API with host buffers ----
-    if lat is not None:
-        lat.close()
     ens = None if args.no_ensemble else ensemble_leg(args)
     clo = None if args.no_closure else closure_leg(args)
     sgl = None if args.no_single else single_leg(args)
     barrier_sync()
-    e2e = None if args.no_e2e else e2e_run(args, p, f, ws)
     state_bytes = 11 * 4 * nodes
     # ---- roofline of the step kernel ----
     peak, peak_kind = peaks()

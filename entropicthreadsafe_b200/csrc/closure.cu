@@ -1072,7 +1072,7 @@ int tslb_attach_closure(tslb_ctx* L, tslb_closure* c, int interval) {
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return tslb_internal::fail(L, TSLB_ERR_CUDA, "closure stream");
     L->closure = c;
     L->closure_interval = interval;
-    return TSLB_OK;
+    return tslb_internal::prepare_step_kernel(L);
 }
 
 const char* tslb_closure_last_error(tslb_closure* c) {

@@ -130,6 +130,12 @@ __global__ void shift_rho_kernel(float* d, long long n) {
     if (i < n) d[i] = d[i] - 1.0f;
 }
 
+// rho = 1 + d into a separate field (the state keeps d)
+__global__ void rho_from_d_kernel(const float* __restrict__ d, float* __restrict__ rho, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) rho[i] = 1.0f + d[i];
+}
+
 // FP32 fields (rho already shifted to rho - 1) -> storage type
 template <class T>
 __global__ void to_storage_kernel(const float* __restrict__ src, T* __restrict__ dst, long long N, long long n, StepArgs a) {
@@ -229,9 +235,8 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const float* __rest
     for (int k = 0; k < RED_SLOTS; ++k) acc[k] = 0.0;
     float umax2 = 0.f;
     const float lo = colour ? -0.9f : 0.1f;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const double d = s[F_D * N + i], rho = 1.0 + d;
-        const double u = s[F_U * N + i], v = s[F_V * N + i], w = s[F_W * N + i], phi = s[F_PHI * N + i];
+    auto node = [&](double d, double u, double v, double w, double phi) {
+        const double rho = 1.0 + d;
         acc[0] += d;  // mass - n, exact for small deviations
         if (colour) { acc[1] += rho * (1.0 + phi) * 0.5; acc[2] += rho * (1.0 - phi) * 0.5; }
         else { acc[1] += phi; acc[2] += 1.0 - phi; }
@@ -241,7 +246,26 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(const float* __rest
         umax2 = fmaxf(umax2, (float)uu);
         if (phi > 0.9) { acc[7] += rho; acc[8] += 1.0; }
         if (phi < lo) { acc[9] += rho; acc[10] += 1.0; }
+    };
+    // four nodes' loads in flight per thread, then their FP64 accumulation
+    constexpr int U4 = 4;
+    const long long S = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + (U4 - 1) * S < n; i += U4 * S) {
+        float x[U4][5];
+#pragma unroll
+        for (int q = 0; q < U4; ++q) {
+            const long long j = i + q * S;
+            x[q][0] = __ldcs(s + F_D * N + j);
+            x[q][1] = __ldcs(s + F_U * N + j);
+            x[q][2] = __ldcs(s + F_V * N + j);
+            x[q][3] = __ldcs(s + F_W * N + j);
+            x[q][4] = __ldcs(s + F_PHI * N + j);
+        }
+#pragma unroll
+        for (int q = 0; q < U4; ++q) node(x[q][0], x[q][1], x[q][2], x[q][3], x[q][4]);
     }
+    for (; i < n; i += S) node(s[F_D * N + i], s[F_U * N + i], s[F_V * N + i], s[F_W * N + i], s[F_PHI * N + i]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // block partials: a fixed shuffle tree per warp, then the warps in order
     for (int k = 0; k < RED_PARTS; ++k) {
@@ -433,38 +457,81 @@ void with_storage(int prec, Fn&& fn) {
 
 int storage_bytes(int prec) { return prec == TSLB_PREC_FP32 ? 4 : 2; }
 
-// every step-kernel instantiation may use the opt-in shared memory it needs
-cudaError_t set_step_attributes() {
-    cudaError_t e = cudaSuccess;
-    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    auto one = [&](auto tag) {
-        using T = decltype(tag);
-        const int es = (int)sizeof(T);
-        const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, es), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, es);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, T>, attr, sc);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, T>, attr, sc);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true, T>, attr, sp);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false, T>, attr, sp);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, true, T>, attr, sp);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, false, T>, attr, sp);
-    };
-    one(float{});
-    one(__nv_bfloat16{});
-    one(__half{});
-    const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, 4), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, 4);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, float, true>, attr, sc);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, float, true>, attr, sc);
-    // interior solids (FP32 storage)
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, true, float, false, true>, attr, sc);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_COLOUR, false, float, false, true>, attr, sc);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true>, attr, sp);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true>, attr, sp);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, true, float, false, true>, attr, sp);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel<TSLB_MODE_SINGLE, false, float, false, true>, attr, sp);
+// The step kernels use more than 48 KB of dynamic shared memory, which needs
+// a function attribute once per kernel and device.  Modules load lazily, so
+// the attribute is set only for the instantiations a lattice launches: at
+// its first launch, or earlier through prepare_step_kernel (before a stream
+// capture, for instance).
+std::mutex g_attr_mu;
+std::vector<std::pair<int, const void*>> g_attr_done;
+
+cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (const auto& d : g_attr_done)
+        if (d.first == dev && d.second == fn) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) g_attr_done.emplace_back(dev, fn);
     return e;
 }
 
+// The lattices' large buffers (state, conversion and output fields, normals)
+// come from one memory pool per device that keeps freed memory for the next
+// lattice: a lattice created after another was destroyed reuses its pages
+// instead of mapping new ones.  Allocation and release are ordered on the
+// lattice's stream.  A failed allocation first returns the pool's cached
+// memory to the device and is tried once more.
+std::mutex g_pool_mu;
+constexpr int MAX_DEVICES = 64;
+cudaMemPool_t g_pool[MAX_DEVICES] = {};
+
+cudaError_t pool_alloc(void** ptr, size_t bytes, int dev, cudaStream_t st) {
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaError_t e = cudaMemPoolCreate(&pool, &props);
+            if (e != cudaSuccess) return e;
+            unsigned long long keep = ~0ULL;
+            e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) {
+                cudaMemPoolDestroy(pool);
+                return e;
+            }
+            g_pool[dev] = pool;
+        }
+        pool = g_pool[dev];
+    }
+    cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, pool, st);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocFromPoolAsync(ptr, bytes, pool, st);
+    }
+    return e;
+}
+
+void pool_free(void* ptr, cudaStream_t st) {
+    if (ptr) cudaFreeAsync(ptr, st);
+}
+
+int ensure_normals(tslb_ctx* c) {
+    if (c->nrm) return TSLB_OK;
+    CUDA_TRY(c, pool_alloc(reinterpret_cast<void**>(&c->nrm), sizeof(float) * 3 * c->N, c->device, c->stream));
+    return TSLB_OK;
+}
+
 int launch_normals(tslb_ctx* c) {
+    int rc = ensure_normals(c);
+    if (rc) return rc;
     StepArgs a = make_args(c, c->state[c->cur], nullptr);
     const int bs = 256;
     const long long grid = (c->n + bs - 1) / bs;
@@ -476,41 +543,43 @@ int launch_normals(tslb_ctx* c) {
     return TSLB_OK;
 }
 
-// the step kernel on one lattice (shared by the context and the no-alloc paths)
-void launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st) {
+// The step kernel on one lattice (shared by the context and the no-alloc
+// paths): the instantiation for the mode, storage, x alignment, tau
+// correction and solid mask of `a`.  launch = false only sets its shared
+// memory attribute.  Returns the error of that attribute; launch errors are
+// left to cudaGetLastError.
+cudaError_t launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st, bool launch = true) {
     dim3 block(TX, TY, 1);
     dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zchunk - 1) / a.zchunk);
+    cudaError_t err = cudaSuccess;
     with_storage(prec, [&](auto tag) {
         using T = decltype(tag);
         const bool vec = a.nx % (16 / (int)sizeof(T)) == 0;
         const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
+        auto go = [&](void (*kernel)(const StepArgs)) {
+            err = ensure_smem_attr((const void*)kernel, sm);
+            if (err == cudaSuccess && launch) kernel<<<grid, block, sm, st>>>(a);
+        };
         if (a.solid && std::is_same<T, float>::value) {
             // interior solid nodes (FP32 storage, no tau correction; checked by tslb_set_solid_mask)
-            if (mode == TSLB_MODE_COLOUR) {
-                if (vec) step_kernel<TSLB_MODE_COLOUR, true, float, false, true><<<grid, block, sm, st>>>(a);
-                else step_kernel<TSLB_MODE_COLOUR, false, float, false, true><<<grid, block, sm, st>>>(a);
-            } else if (mode == TSLB_MODE_SINGLE) {
-                if (vec) step_kernel<TSLB_MODE_SINGLE, true, float, false, true><<<grid, block, sm, st>>>(a);
-                else step_kernel<TSLB_MODE_SINGLE, false, float, false, true><<<grid, block, sm, st>>>(a);
-            } else {
-                if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true><<<grid, block, sm, st>>>(a);
-                else step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true><<<grid, block, sm, st>>>(a);
-            }
+            if (mode == TSLB_MODE_COLOUR) go(vec ? step_kernel<TSLB_MODE_COLOUR, true, float, false, true>
+                                                 : step_kernel<TSLB_MODE_COLOUR, false, float, false, true>);
+            else if (mode == TSLB_MODE_SINGLE) go(vec ? step_kernel<TSLB_MODE_SINGLE, true, float, false, true>
+                                                      : step_kernel<TSLB_MODE_SINGLE, false, float, false, true>);
+            else go(vec ? step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true>
+                        : step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true>);
         } else if (mode == TSLB_MODE_COLOUR && a.dtau && std::is_same<T, float>::value) {
             // per-node tau correction (FP32 storage only; checked by the callers)
-            if (vec) step_kernel<TSLB_MODE_COLOUR, true, float, true><<<grid, block, sm, st>>>(a);
-            else step_kernel<TSLB_MODE_COLOUR, false, float, true><<<grid, block, sm, st>>>(a);
+            go(vec ? step_kernel<TSLB_MODE_COLOUR, true, float, true> : step_kernel<TSLB_MODE_COLOUR, false, float, true>);
         } else if (mode == TSLB_MODE_COLOUR) {
-            if (vec) step_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, st>>>(a);
-            else step_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, st>>>(a);
+            go(vec ? step_kernel<TSLB_MODE_COLOUR, true, T> : step_kernel<TSLB_MODE_COLOUR, false, T>);
         } else if (mode == TSLB_MODE_SINGLE) {
-            if (vec) step_kernel<TSLB_MODE_SINGLE, true, T><<<grid, block, sm, st>>>(a);
-            else step_kernel<TSLB_MODE_SINGLE, false, T><<<grid, block, sm, st>>>(a);
+            go(vec ? step_kernel<TSLB_MODE_SINGLE, true, T> : step_kernel<TSLB_MODE_SINGLE, false, T>);
         } else {
-            if (vec) step_kernel<TSLB_MODE_PHASEFIELD, true, T><<<grid, block, sm, st>>>(a);
-            else step_kernel<TSLB_MODE_PHASEFIELD, false, T><<<grid, block, sm, st>>>(a);
+            go(vec ? step_kernel<TSLB_MODE_PHASEFIELD, true, T> : step_kernel<TSLB_MODE_PHASEFIELD, false, T>);
         }
     });
+    return err;
 }
 
 int launch_moment_bcs(tslb_ctx* c) {
@@ -545,7 +614,7 @@ int launch_step(tslb_ctx* c) {
         if (rc) return rc;
     }
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    launch_step_kernel(a, c->p.mode, c->p.precision, c->stream);
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream));
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
@@ -611,6 +680,12 @@ int ensure_dtau(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+int prepare_step_kernel(tslb_ctx* c) {
+    StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, false));
+    return TSLB_OK;
+}
+
 }  // namespace tslb_internal
 
 namespace {
@@ -671,10 +746,22 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     c->esize = storage_bytes(p->precision);
     default_scales(c);
     for (int b = 0; b < 2; ++b)
-        if ((e = cudaMalloc(&c->state[b], (size_t)c->esize * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(state)");
+        if ((e = pool_alloc(&c->state[b], (size_t)c->esize * NF * c->N, c->device, c->stream)) != cudaSuccess)
+            return bail(e, "allocation (state)");
     if (p->precision != TSLB_PREC_FP32)
-        if ((e = cudaMalloc(&c->io, sizeof(float) * NF * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(io)");
-    if ((e = cudaMalloc(&c->nrm, sizeof(float) * 3 * c->N)) != cudaSuccess) return bail(e, "cudaMalloc(normals)");
+        if ((e = pool_alloc(reinterpret_cast<void**>(&c->io), sizeof(float) * NF * c->N, c->device, c->stream)) != cudaSuccess)
+            return bail(e, "allocation (io)");
+    // rho = 1 + d for downloads (with the lattice, so lattices of one size
+    // allocate alike and reuse each other's pool memory)
+    if ((e = pool_alloc(reinterpret_cast<void**>(&c->rho_out), sizeof(float) * c->N, c->device, c->stream)) != cudaSuccess)
+        return bail(e, "allocation (rho)");
+    // interface normals: a field of the phase-field step; colour mode only
+    // forms them for tslb_download_normals (allocated then)
+    if (p->mode == TSLB_MODE_PHASEFIELD)
+        if ((e = pool_alloc(reinterpret_cast<void**>(&c->nrm), sizeof(float) * 3 * c->N, c->device, c->stream)) != cudaSuccess)
+            return bail(e, "allocation (normals)");
+    // the pool's allocations are ordered on the lattice's stream: complete them for every stream
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
     if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
     {
         int sm_count = 148;
@@ -693,7 +780,6 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
         if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
     }
-    if ((e = set_step_attributes()) != cudaSuccess) return bail(e, "cudaFuncSetAttribute");
     // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -701,6 +787,8 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     long long want = 8LL * sms;
     int zc = (int)std::max<long long>(8, (tiles * nz + want - 1) / want);
     c->zchunk = std::min(zc, nz);
+    if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false)) != cudaSuccess)
+        return bail(e, "cudaFuncSetAttribute");
     *out = c;
     return TSLB_OK;
 }
@@ -708,9 +796,11 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
 void tslb_destroy(tslb_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int b = 0; b < 2; ++b) cudaFree(c->state[b]);
-    cudaFree(c->io);
-    cudaFree(c->nrm);
+    for (int b = 0; b < 2; ++b) pool_free(c->state[b], c->stream);
+    pool_free(c->io, c->stream);
+    pool_free(c->rho_out, c->stream);
+    pool_free(c->nrm, c->stream);
+    if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->flags);
     cudaFree(c->red);
     cudaFreeHost(c->red_host);
@@ -824,11 +914,20 @@ int tslb_download_moments(tslb_ctx* c, float* rho, float* u, float* v, float* w,
     const float* s = nullptr;
     int rc = fp32_view(c, &s);
     if (rc) return rc;
-    for (int f = 0; f < NF; ++f)
-        if (dst[f]) CUDA_TRY(c, cudaMemcpyAsync(dst[f], s + f * c->N, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    for (int f = 0; f < NF; ++f) {
+        if (!dst[f]) continue;
+        const float* src = s + f * c->N;
+        if (f == F_D) {
+            // the state holds d = rho - 1: rho is formed on the device
+            const int bs = 256;
+            rho_from_d_kernel<<<(unsigned)((c->n + bs - 1) / bs), bs, 0, c->stream>>>(src, c->rho_out, c->n);
+            c->launches++;
+            CUDA_TRY(c, cudaGetLastError());
+            src = c->rho_out;
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(dst[f], src, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (rho)
-        for (long long i = 0; i < c->n; ++i) rho[i] = 1.0f + rho[i];
     return check_flags(c);
 }
 
@@ -945,7 +1044,7 @@ int tslb_set_solid_mask(tslb_ctx* c, const unsigned char* isfluid) {
     cudaFree(d);
     if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string("tslb_set_solid_mask: ") + cudaGetErrorString(e));
     c->solid_on = true;
-    return TSLB_OK;
+    return tslb_internal::prepare_step_kernel(c);
 }
 
 int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
@@ -965,7 +1064,7 @@ int tslb_set_tau_correction(tslb_ctx* c, const float* dtau) {
     CUDA_TRY(c, cudaMemcpyAsync(c->dtau_base, dtau, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->base_on = true;
-    return TSLB_OK;
+    return tslb_internal::prepare_step_kernel(c);
 }
 
 int tslb_download_tau_correction(tslb_ctx* c, float* dtau) {
@@ -1163,8 +1262,6 @@ int noalloc_setup(int dev, NoallocScratch** out) {
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(normals): ") + cudaGetErrorString(e));
         e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(flags): ") + cudaGetErrorString(e));
-        if ((e = set_step_attributes()) != cudaSuccess)
-            return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
         s.ready = true;
     }
     *out = &s;
@@ -1221,7 +1318,8 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
         if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("normals launch: ") + cudaGetErrorString(e));
     }
     StepArgs a = make_args(&view, d_in, d_out);
-    launch_step_kernel(a, p->mode, TSLB_PREC_FP32, st);
+    if ((e = launch_step_kernel(a, p->mode, TSLB_PREC_FP32, st)) != cudaSuccess)
+        return noalloc_fail(TSLB_ERR_CUDA, std::string("step kernel attribute: ") + cudaGetErrorString(e));
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
     return TSLB_OK;
 }
@@ -1298,6 +1396,25 @@ int ens_build(tslb_ensemble* e) {
     return TSLB_OK;
 }
 
+// The ensemble kernel of the ensemble's mode, storage and x alignment:
+// sets its shared-memory attribute and (launch) launches one step.
+cudaError_t ens_kernel(tslb_ensemble* e, bool launch) {
+    const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
+    const StepArgs* args = e->d_args[e->parity];
+    cudaError_t err = cudaSuccess;
+    with_storage(e->precision, [&](auto tag) {
+        using T = decltype(tag);
+        const size_t sm = step_smem_bytes_es(e->mode, (int)sizeof(T));
+        auto go = [&](void (*kernel)(const StepArgs*, const WorkItem*, int)) {
+            err = ensure_smem_attr((const void*)kernel, sm);
+            if (err == cudaSuccess && launch) kernel<<<grid, dim3(TX, TY, 1), sm, e->stream>>>(args, e->d_work, e->nwork);
+        };
+        if (e->mode == TSLB_MODE_COLOUR) go(e->vec ? ensemble_kernel<TSLB_MODE_COLOUR, true, T> : ensemble_kernel<TSLB_MODE_COLOUR, false, T>);
+        else go(e->vec ? ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T> : ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T>);
+    });
+    return err;
+}
+
 // one ensemble step on the ensemble stream (no host synchronisation)
 int ens_launch(tslb_ensemble* e) {
     if (e->mode == TSLB_MODE_PHASEFIELD) {
@@ -1309,20 +1426,7 @@ int ens_launch(tslb_ensemble* e) {
             });
         }
     }
-    const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
-    const StepArgs* args = e->d_args[e->parity];
-    with_storage(e->precision, [&](auto tag) {
-        using T = decltype(tag);
-        const size_t sm = step_smem_bytes_es(e->mode, (int)sizeof(T));
-        dim3 block(TX, TY, 1);
-        if (e->mode == TSLB_MODE_COLOUR) {
-            if (e->vec) ensemble_kernel<TSLB_MODE_COLOUR, true, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
-            else ensemble_kernel<TSLB_MODE_COLOUR, false, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
-        } else {
-            if (e->vec) ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
-            else ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T><<<grid, block, sm, e->stream>>>(args, e->d_work, e->nwork);
-        }
-    });
+    ECUDA_TRY(e, ens_kernel(e, true));
     ECUDA_TRY(e, cudaGetLastError());
     e->parity ^= 1;
     return TSLB_OK;
@@ -1336,24 +1440,6 @@ void ens_settle(tslb_ensemble* e) {
         std::swap(e->d_args[0], e->d_args[1]);
         e->parity = 0;
     }
-}
-
-cudaError_t ens_set_attributes() {
-    cudaError_t err = cudaSuccess;
-    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    auto one = [&](auto tag) {
-        using T = decltype(tag);
-        const int es = (int)sizeof(T);
-        const int sc = (int)step_smem_bytes_es(TSLB_MODE_COLOUR, es), sp = (int)step_smem_bytes_es(TSLB_MODE_PHASEFIELD, es);
-        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_COLOUR, true, T>, attr, sc);
-        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_COLOUR, false, T>, attr, sc);
-        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T>, attr, sp);
-        if (err == cudaSuccess) err = cudaFuncSetAttribute(ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T>, attr, sp);
-    };
-    one(float{});
-    one(__nv_bfloat16{});
-    one(__half{});
-    return err;
 }
 
 int ens_check(tslb_ensemble* e, int i) {
@@ -1396,7 +1482,7 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         if (dims[3 * i] % epc) e->vec = false;
     }
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
-    if (ce == cudaSuccess) ce = ens_set_attributes();
+    if (ce == cudaSuccess) ce = ens_kernel(e, false);
     int dev = 0;
     if (ce == cudaSuccess) ce = cudaGetDevice(&dev);
     if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, dev);

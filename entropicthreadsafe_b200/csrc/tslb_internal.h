@@ -21,6 +21,7 @@ struct tslb_ctx {
     void* state[2] = {nullptr, nullptr};   // ping-pong, 11 fields each, storage type
     int esize = 4;                         // bytes per stored element
     float* io = nullptr;                   // FP32 conversion buffer (bf16/fp16 storage)
+    float* rho_out = nullptr;              // rho = 1 + d for downloads
     float scale[tslb::NF];                 // fp16 storage: stored = value * scale
     int cur = 0;
     float* nrm = nullptr;                  // 3 fields
@@ -67,4 +68,7 @@ int fp32_view(tslb_ctx* c, const float** out);
 int ensure_dtau(tslb_ctx* c);
 // closure.cu: refresh c->dtau from the attached closure before a step
 int closure_before_step(tslb_ctx* c);
+// set the shared-memory attribute of the step kernel the context launches
+// next (its mode, storage, tau correction and solid mask)
+int prepare_step_kernel(tslb_ctx* c);
 }  // namespace tslb_internal
