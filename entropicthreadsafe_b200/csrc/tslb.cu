@@ -529,6 +529,29 @@ int ensure_normals(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+// Target planes per block.  Each chunk also reads the source planes just
+// outside it, so long chunks repeat less work; the chunks per tile column
+// are the fewest whose blocks fill the resident slots (two blocks per SM) in
+// whole waves to at least 90%, with chunks of at least 8 planes.
+int choose_zchunk(long long tiles, int nz, int sms) {
+    const long long slots = 2LL * sms;
+    const int max_chunks = std::max(1, nz / 8);
+    int best = 1;
+    double best_fill = -1.0;
+    for (int nc = 1; nc <= max_chunks; ++nc) {
+        const int zc = (nz + nc - 1) / nc;
+        const long long blocks = tiles * ((nz + zc - 1) / zc);
+        const long long waves = (blocks + slots - 1) / slots;
+        const double fill = (double)blocks / (double)(waves * slots);
+        if (fill > best_fill + 1e-9) {
+            best_fill = fill;
+            best = nc;
+        }
+        if (fill >= 0.9) break;
+    }
+    return (nz + best - 1) / best;
+}
+
 int launch_normals(tslb_ctx* c) {
     int rc = ensure_normals(c);
     if (rc) return rc;
@@ -780,13 +803,9 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
         if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
     }
-    // z chunk: enough blocks for ~4 waves of 2 blocks per SM, at least 8 planes
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
-    long long want = 8LL * sms;
-    int zc = (int)std::max<long long>(8, (tiles * nz + want - 1) / want);
-    c->zchunk = std::min(zc, nz);
+    c->zchunk = choose_zchunk((long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY), nz, sms);
     if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false)) != cudaSuccess)
         return bail(e, "cudaFuncSetAttribute");
     *out = c;

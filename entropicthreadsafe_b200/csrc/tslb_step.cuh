@@ -403,6 +403,9 @@ __device__ __forceinline__ void cp_async16(float* sdst, const float* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async16s(unsigned sa, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -481,6 +484,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         pch_out = nd.out;
         pch_dst = row * SW + EPC * ch;
     }
+    const T* pg0 = gin + F_PHI * a.N + pch_off;
+    const unsigned ps0 = (unsigned)__cvta_generic_to_shared(phis) + (unsigned)(pch_dst * sizeof(T));
     auto ghost = [&](float v) { return cvt_out<T>(v, a, F_PHI); };
     auto stage_phi = [&](int z) {
         bool zout;
@@ -491,7 +496,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
             if (tid < G::PCOPIES) {
                 T* dst = slot + pch_dst;
                 if (!pch_out && !zout) {
-                    cp_async16(reinterpret_cast<float*>(dst), reinterpret_cast<const float*>(ph + pch_off));
+                    cp_async16s(ps0 + (unsigned)((z & 3) * (PAREA * (int)sizeof(T))), pg0 + (long long)gz * plane);
                 } else {
                     const int row = tid / G::NCH, ch = tid % G::NCH;
 #pragma unroll
@@ -530,6 +535,11 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         mcell_ok = !nd.out;
         mcell_dst = mfg * MAREA + row * SW + EPC * ch;
     }
+    // per-thread staging bases: global (field group, cell) and shared (cell)
+    const T* mg0 = gin + mfg * a.N + mcell_off;
+    const long long mfstride = (long long)G::MGROUPS * a.N;
+    const unsigned ms0 = (unsigned)__cvta_generic_to_shared(mst) + (unsigned)(mcell_dst * sizeof(T));
+
     auto stage_mom = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
@@ -538,13 +548,12 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         const T* src = gin + (long long)gz * plane;
         if (VEC) {
             if (mcell_ok) {
-                T* d = dst + mcell_dst;
-                const T* g = src + mfg * a.N + mcell_off;
+                const unsigned d = ms0 + (unsigned)((z & 1) * (NMOM * MAREA * (int)sizeof(T)));
+                const T* g = mg0 + (long long)gz * plane;
 #pragma unroll
                 for (int k = 0; k < G::MFIELDS; ++k) {
                     if (G::MGROUPS * G::MFIELDS == NMOM || mfg + k * G::MGROUPS < NMOM)
-                        cp_async16(reinterpret_cast<float*>(d + k * G::MGROUPS * MAREA),
-                                   reinterpret_cast<const float*>(g + k * G::MGROUPS * a.N));
+                        cp_async16s(d + (unsigned)(k * G::MGROUPS * MAREA * (int)sizeof(T)), g + k * mfstride);
                 }
             }
         } else {
