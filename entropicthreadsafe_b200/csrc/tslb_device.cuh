@@ -32,13 +32,23 @@ namespace tslb {
 constexpr int NF = 11;
 enum { F_D = 0, F_U, F_V, F_W, F_XX, F_XY, F_XZ, F_YY, F_YZ, F_ZZ, F_PHI };
 
-// coefficient slots (per node, shared memory)
+// Coefficient slots (per node, shared memory), ordered in pairs that the
+// pull always reads together, so each pair is one 8-byte load:
+//   (0, z), (zz, c0)       every source
+//   (x, xx), (xz, xxz), (xzz, c1)   sources with cx != 0
+//   (y, yy), (yz, yyz), (yzz, c2)   sources with cy != 0
+//   (xy, xyz), (xxy, xyy)           sources with cx != 0 and cy != 0
+//   (c3, c4)                        every source (c4: the rest population's)
+// Colour slots c0..c4: phi, Bx, By, Bz, delta0 | phase field: G0, G1x, G1y, G1z, -.
 enum {
-    K_0 = 0, K_X, K_Y, K_Z, K_XX, K_YY, K_ZZ, K_XY, K_XZ, K_YZ,
-    K_XXY, K_XXZ, K_XYY, K_YYZ, K_XZZ, K_YZZ, K_XYZ,
-    K_C0, K_C1, K_C2, K_C3, K_C4,   // colour: phi, Bx, By, Bz, delta0 | phase field: G0, G1x, G1y, G1z, -
+    K_0 = 0, K_Z, K_ZZ, K_C0,
+    K_X, K_XX, K_XZ, K_XXZ, K_XZZ, K_C1,
+    K_Y, K_YY, K_YZ, K_YYZ, K_YZZ, K_C2,
+    K_XY, K_XYZ, K_XXY, K_XYY,
+    K_C3, K_C4,
     NCOEF
 };
+static_assert(NCOEF % 2 == 0, "coefficient slots come in pairs");
 
 // accumulator slots of a target node
 enum { A_RHO = 0, A_JX, A_JY, A_JZ, A_XX, A_XY, A_XZ, A_YY, A_YZ, A_ZZ, A_COL, NACC };
@@ -375,6 +385,8 @@ __device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, co
         // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta; n = 0 off the interface)
         const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
         K[K_C0] = phi; K[K_C1] = bb * nx_; K[K_C2] = bb * ny_; K[K_C3] = bb * nz_; K[K_C4] = d0;
+    } else if (MODE == TSLB_MODE_SINGLE) {
+        K[K_C0] = 0.f; K[K_C1] = 0.f; K[K_C2] = 0.f; K[K_C3] = 0.f; K[K_C4] = 0.f;
     } else if (MODE == TSLB_MODE_PHASEFIELD) {
         // D3Q7 phase field: g_q = G0 + e_q.G1 (recursive_2c_TSLB3D.f90:808-831)
         const float sh = 0.125f * a.sharp * phi * (1.f - phi);

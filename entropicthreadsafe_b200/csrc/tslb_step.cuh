@@ -26,14 +26,20 @@
 
 namespace tslb {
 
-// Coefficients live in shared memory as NCOEF scalar planes of CAREA floats
-// (slot-major), so each source loads exactly the slots its directions use.
-// (single-component mode has no colour slots)
+// Coefficients live in shared memory as NCOEF/2 planes of CAREA float2
+// (slot pairs, pair-major): node n's pair p is at float offset
+// p * 2 CAREA + 2 n.  Each source loads the pairs its directions use, one
+// 8-byte load per pair; lanes (consecutive x) read consecutive 8-byte words.
+__device__ __forceinline__ float coef_at(const float* Kn, int slot) {
+    const float2 v = *reinterpret_cast<const float2*>(Kn + (slot >> 1) * (2 * CAREA));
+    return (slot & 1) ? v.y : v.x;
+}
+// (single-component mode leaves the colour slots unset: stored, never read)
 template <int MODE>
 __device__ __forceinline__ void store_coefs(float* dst, const float* K) {
-    constexpr int n = MODE == TSLB_MODE_SINGLE ? K_C0 : NCOEF;
 #pragma unroll
-    for (int c = 0; c < n; ++c) dst[c * CAREA] = K[c];
+    for (int p = 0; p < NCOEF / 2; ++p)
+        *reinterpret_cast<float2*>(dst + p * (2 * CAREA)) = make_float2(K[2 * p], K[2 * p + 1]);
 }
 
 // P' = Q0 + cz Q1 + cz^2 Q2 of the directions (CXv, CYv, cz), cz = -1, 0, 1,
@@ -41,7 +47,7 @@ __device__ __forceinline__ void store_coefs(float* dst, const float* K) {
 template <int CXv, int CYv>
 struct Src {
     const float* Kp;
-    __device__ __forceinline__ float L(int slot) const { return Kp[slot * CAREA]; }
+    __device__ __forceinline__ float L(int slot) const { return coef_at(Kp, slot); }
     __device__ __forceinline__ void eval(float& Pm, float& P0, float& Pp) const {
         float q0 = L(K_0);
         if (CXv) q0 += CXv * L(K_X) + L(K_XX);
@@ -68,7 +74,7 @@ template <int CYv>
 struct SrcPair {
     const float* Ka;   // source of cx = +1
     const float* Kb;   // source of cx = -1
-    __device__ __forceinline__ float2 L(int slot) const { return make_float2(Ka[slot * CAREA], Kb[slot * CAREA]); }
+    __device__ __forceinline__ float2 L(int slot) const { return make_float2(coef_at(Ka, slot), coef_at(Kb, slot)); }
     __device__ __forceinline__ void eval(float2& Pm, float2& P0, float2& Pp) const {
         const float2 sx = make_float2(1.f, -1.f);
         float2 q0 = __fadd2_rn(L(K_0), __ffma2_rn(sx, L(K_X), L(K_XX)));
@@ -135,9 +141,9 @@ __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float 
 template <int MODE, int CYv>
 __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp,
                                          float phm, float ph0, float php) {
-    const Src<1, CYv> sa{Kc - CYv * CW - 1};   // source of cx = +1 (x - 1)
-    const Src<0, CYv> sz{Kc - CYv * CW};       // source of cx = 0
-    const Src<-1, CYv> sb{Kc - CYv * CW + 1};  // source of cx = -1 (x + 1)
+    const Src<1, CYv> sa{Kc - 2 * (CYv * CW + 1)};   // source of cx = +1 (x - 1)
+    const Src<0, CYv> sz{Kc - 2 * (CYv * CW)};       // source of cx = 0
+    const Src<-1, CYv> sb{Kc - 2 * (CYv * CW - 1)};  // source of cx = -1 (x + 1)
     float am, a0, ap, cm, c0, cp, bm, b0, bp;
     {
         float2 pm, p0, pp;
@@ -188,7 +194,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                                 float* acc) {
     float Kp[NCOEF];
 #pragma unroll
-    for (int c = 0; c < (MODE == TSLB_MODE_SINGLE ? (int)K_C0 : NCOEF); ++c) Kp[c] = Kc[c * CAREA];
+    for (int c = 0; c < NCOEF; ++c) Kp[c] = coef_at(Kc, c);
     // colour mode accumulates colour increments over the target's own phi
     const float pht = Kp[K_C0];
     // own raw moments (velocity faces only)
@@ -636,13 +642,13 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 }
                 node_coefs<MODE, TAU>(a, m, g, gx, gy, gz, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
-            store_coefs<MODE>(coef + ci, K);
+            store_coefs<MODE>(coef + 2 * ci, K);
         }
         cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
         // ---- 2. pull ----
         if (active) {
-            const float* Kc = coef + (ty + 1) * CW + (tx + 1);
+            const float* Kc = coef + 2 * ((ty + 1) * CW + (tx + 1));
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
                 // own-column phi of the target planes (the ring holds planes s-1 .. s+2)
