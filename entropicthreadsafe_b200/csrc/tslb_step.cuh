@@ -608,10 +608,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         const int gz = zwrap(s, zsolid);
         const T* ms = mst + (s & 1) * (NMOM * MAREA);
         // a solid source plane sends nothing: no coefficients, no pull
-        for (int r = 0; r < (zsolid ? 0 : nnodes); ++r) {
-            const XYNode nd = r ? cn1 : cn0;
-            const int ci = r ? ci1 : ci0;
-            const int mi = r ? mi1 : mi0;
+        auto coef_node = [&](const XYNode& nd, const int ci, const int mi, const int pi) {
             float K[NCOEF];
             // solid nodes (behind a face, or interior solids) send nothing
             if (nd.out || (SOLID && bit_at(a.solid, (long long)gz * plane + nd.off))) {
@@ -624,7 +621,6 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 float g[3] = {0.f, 0.f, 0.f};
                 int gx = 0, gy = 0;
                 if (MODE == TSLB_MODE_COLOUR) {
-                    const int pi = r ? pi1 : pi0;
                     const T* p0 = phis + (s & 3) * PAREA + pi;
                     const T* pm = phis + ((s - 1) & 3) * PAREA + pi;
                     const T* pp = phis + ((s + 1) & 3) * PAREA + pi;
@@ -643,6 +639,10 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 node_coefs<MODE, TAU>(a, m, g, gx, gy, gz, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs<MODE>(coef + 2 * ci, K);
+        };
+        if (!zsolid) {
+            coef_node(cn0, ci0, mi0, pi0);
+            if (has_rim) coef_node(cn1, ci1, mi1, pi1);
         }
         cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
