@@ -350,9 +350,13 @@ struct Geo {
     static constexpr int PEROUNDS = (PELEMS + NTHR - 1) / NTHR;
 };
 
+// Phi ring: slot z & (PRING - 1) holds phi plane z.  Iteration s stages plane
+// s+2 while other threads may still read plane s-2 (the previous iteration's
+// target plane s-2 in its pull), so the ring holds at least 5 planes.
+constexpr int PRING = 8;
 __host__ __device__ constexpr size_t step_smem_bytes_es(int mode, int es) {
     return sizeof(float) * 2 * NCOEF * CAREA + (size_t)es * 2 * NMOM * CH * (TX + 2 * (16 / es)) +
-           (mode == TSLB_MODE_COLOUR ? (size_t)es * 4 * (TY + 4) * (TX + 2 * (16 / es)) : 0);
+           (mode == TSLB_MODE_COLOUR ? (size_t)es * PRING * (TY + 4) * (TX + 2 * (16 / es)) : 0);
 }
 __host__ __device__ constexpr size_t step_smem_bytes(int mode) { return step_smem_bytes_es(mode, 4); }
 
@@ -428,7 +432,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     extern __shared__ float4 smem4[];
     float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NCOEF][CAREA]
     T* mst = reinterpret_cast<T*>(coef_base + 2 * NCOEF * CAREA);     // [2][NMOM][MROWS][SW]
-    T* phis = mst + 2 * NMOM * MAREA;                                 // colour: [4][PROWS][SW]
+    T* phis = mst + 2 * NMOM * MAREA;                                 // colour: [PRING][PROWS][SW]
     const T* gin = reinterpret_cast<const T*>(a.in);
     T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -496,13 +500,13 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     auto stage_phi = [&](int z) {
         bool zout;
         const int gz = zwrap(z, zout);
-        T* slot = phis + (z & 3) * PAREA;
+        T* slot = phis + (z & (PRING - 1)) * PAREA;
         const T* ph = gin + F_PHI * a.N + (long long)gz * plane;
         if (VEC) {
             if (tid < G::PCOPIES) {
                 T* dst = slot + pch_dst;
                 if (!pch_out && !zout) {
-                    cp_async16s(ps0 + (unsigned)((z & 3) * (PAREA * (int)sizeof(T))), pg0 + (long long)gz * plane);
+                    cp_async16s(ps0 + (unsigned)((z & (PRING - 1)) * (PAREA * (int)sizeof(T))), pg0 + (long long)gz * plane);
                 } else {
                     const int row = tid / G::NCH, ch = tid % G::NCH;
 #pragma unroll
@@ -621,9 +625,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 float g[3] = {0.f, 0.f, 0.f};
                 int gx = 0, gy = 0;
                 if (MODE == TSLB_MODE_COLOUR) {
-                    const T* p0 = phis + (s & 3) * PAREA + pi;
-                    const T* pm = phis + ((s - 1) & 3) * PAREA + pi;
-                    const T* pp = phis + ((s + 1) & 3) * PAREA + pi;
+                    const T* p0 = phis + (s & (PRING - 1)) * PAREA + pi;
+                    const T* pm = phis + ((s - 1) & (PRING - 1)) * PAREA + pi;
+                    const T* pp = phis + ((s + 1) & (PRING - 1)) * PAREA + pi;
                     m[F_PHI] = cvt_in<T>(*p0, a, F_PHI);
                     grad_smem<SW>(pm, p0, pp, g);
                     if constexpr (std::is_same<T, __half>::value) {
@@ -651,11 +655,11 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
             const float* Kc = coef + 2 * ((ty + 1) * CW + (tx + 1));
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
-                // own-column phi of the target planes (the ring holds planes s-1 .. s+2)
+                // own-column phi of the target planes s-1 .. s+1
                 const int po = (ty + 2) * SW + (tx + EPC);
-                phm = cvt_in<T>(phis[((s - 1) & 3) * PAREA + po], a, F_PHI);
-                ph0 = cvt_in<T>(phis[(s & 3) * PAREA + po], a, F_PHI);
-                php = cvt_in<T>(phis[((s + 1) & 3) * PAREA + po], a, F_PHI);
+                phm = cvt_in<T>(phis[((s - 1) & (PRING - 1)) * PAREA + po], a, F_PHI);
+                ph0 = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + po], a, F_PHI);
+                php = cvt_in<T>(phis[((s + 1) & (PRING - 1)) * PAREA + po], a, F_PHI);
             }
             if (!zsolid) {
                 pull_row<MODE, -1>(Kc, accm, acc0, accp, phm, ph0, php);

@@ -171,6 +171,32 @@ def test_odd_sizes_partial_tiles():
     assert_parity(gpu, o64, o32, "odd sizes")
 
 
+@pytest.mark.parametrize("walls", ["periodic", "bounceback_xy"])
+def test_row_staging_partial_tiles(walls):
+    """nx = 44, a multiple of the 16-byte chunk: planes are staged in 16-byte
+    chunks.  The second x tile is partial; with periodic faces its staged rows
+    wrap around the x faces, with walls the chunks behind the x and y faces are
+    ghost values."""
+    p, _ = workloads.droplet(n=24, radius=5.0)
+    nx, ny, nz = 44, 12, 16
+    f = workloads.empty_fields(nx, ny, nz)
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    # a droplet across the boundary of the two x tiles, and velocity noise
+    r = np.sqrt((x - 31.5) ** 2 + (y - 5.5) ** 2 + (z - 7.5) ** 2)
+    f["phi"][:] = np.tanh((4.5 - r) / 1.5)
+    rng = np.random.default_rng(5)
+    for k in ("u", "v", "w"):
+        f[k][:] = rng.normal(0.0, 0.01, f[k].shape)
+    if walls != "periodic":
+        for face in (capi.FACE_XM, capi.FACE_XP, capi.FACE_YM, capi.FACE_YP):
+            p.bc[face] = capi.BC_BOUNCEBACK
+            p.bc_phi[face] = -1.0
+    gpu, _ = run_gpu(p, f, 30)
+    o64, _ = run_oracle(p, f, 30, fp64=True)
+    o32, _ = run_oracle(p, f, 30, fp64=False)
+    assert_parity(gpu, o64, o32, f"row staging, {walls}")
+
+
 def test_reduce_is_exact_and_matches_oracle():
     """tslb_reduce (FP64 on the device) against numpy FP64 sums of the same
     downloaded state, and against the oracle's diagnostics at FP32 level."""
