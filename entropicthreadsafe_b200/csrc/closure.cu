@@ -48,7 +48,8 @@ struct tslb_closure {
     std::string err;
 };
 
-static std::string g_closure_create_error;
+// message of this thread's last failed tslb_closure_create (per thread)
+static thread_local std::string g_closure_create_error;
 
 namespace {
 

@@ -19,7 +19,9 @@
 
 using namespace tslb;
 
-static std::string g_create_error;
+// message of this thread's last failed creation (tslb_create, tslb_ensemble_create,
+// tslb_step_noalloc): per thread, so concurrent failures do not race
+static thread_local std::string g_create_error;
 
 namespace tslb_internal {
 

@@ -259,7 +259,9 @@ void* tslb_stream(tslb_ctx* ctx);
 long long tslb_launch_count(tslb_ctx* ctx);
 
 /* Message of the last failed call on ctx (or, when ctx is NULL, of the
- * last failed tslb_create or tslb_step_noalloc).  Never NULL. */
+ * calling thread's last failed tslb_create or tslb_step_noalloc: each host
+ * thread keeps its own).  Never NULL.  A context is used by one thread at a
+ * time; different contexts may be used by different threads concurrently. */
 const char* tslb_last_error(tslb_ctx* ctx);
 
 /* ---- batched ensemble of independent lattices ----

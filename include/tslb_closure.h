@@ -118,6 +118,8 @@ int  tslb_closure_features(tslb_closure* c, tslb_ctx* lattice, float* features);
  * attached closure while the lattice's stream has work queued. */
 int  tslb_attach_closure(tslb_ctx* lattice, tslb_closure* c, int interval);
 
+/* Message of the last failed call on c (or, when c is NULL, of the calling
+ * thread's last failed tslb_closure_create).  Never NULL. */
 const char* tslb_closure_last_error(tslb_closure* c);
 
 #ifdef __cplusplus
