@@ -44,7 +44,7 @@ def _stale() -> bool:
 def build_driver() -> str:
     """The host driver tslb_run (C++), linked against libtslb.so next to it."""
     cxx = os.environ.get("CXX_DRIVER", "g++")
-    cmd = [cxx, "-O2", "-std=c++17", "-o", DRIVER, DRIVER_SRC, "-L" + HERE, "-ltslb", "-Wl,-rpath,$ORIGIN"]
+    cmd = [cxx, "-O2", "-std=c++17", "-pthread", "-o", DRIVER, DRIVER_SRC, "-L" + HERE, "-ltslb", "-Wl,-rpath,$ORIGIN"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("driver build failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)

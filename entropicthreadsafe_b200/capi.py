@@ -214,7 +214,9 @@ def lib() -> ctypes.CDLL:
                                 ("tslb_frame_path", [ctypes.c_char_p, ip, cp, cp, cp, ip, cp], ip),
                                 ("tslb_checkpoint_save", [vp, cp], ip),
                                 ("tslb_checkpoint_load", [vp, cp], ip),
-                                ("tslb_steps_done", [vp], ctypes.c_longlong)):
+                                ("tslb_steps_done", [vp], ctypes.c_longlong),
+                                ("tslb_host_alloc", [ctypes.c_longlong], vp),
+                                ("tslb_host_free", [vp], None)):
             getattr(L, name).argtypes = args
             getattr(L, name).restype = res
         _lib = L

@@ -952,6 +952,20 @@ int tslb_download_moments(tslb_ctx* c, float* rho, float* u, float* v, float* w,
     return check_flags(c);
 }
 
+void* tslb_host_alloc(long long bytes) {
+    if (bytes <= 0) return nullptr;
+    void* p = nullptr;
+    if (cudaMallocHost(&p, (size_t)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void tslb_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
 int tslb_download_normals(tslb_ctx* c, float* nx, float* ny, float* nz) {
     if (!c) return TSLB_ERR_ARG;
     if (!c->loaded) return fail(c, TSLB_ERR_STATE, "download before an upload");

@@ -13,6 +13,11 @@
 // the reference's throughput line, glups = nx ny nz nsteps / 1e9 / wall
 // seconds (:844), and the same over the stepping alone.
 //
+// Frames and slices are written asynchronously: the fields are downloaded
+// into host buffers of their own and a writer thread writes the files while
+// the lattice keeps stepping (at most two frames in flight).  Checkpoints are
+// written synchronously.  The wall time includes waiting for the last write.
+//
 // Workloads: "droplet" is the static droplet of config 1 (colour mode,
 // periodic n^3 box, R = n/4, tau 0.8, sigma 0.01, beta 0.7, phi =
 // tanh((R - r)/2)); "jet" is the round jet of config 5 (192 x 192 x 384
@@ -22,6 +27,12 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -80,6 +91,60 @@ int check(tslb_ctx* ctx, int rc, const char* what) {
 double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+// One thread that runs file-writing jobs in order; the first failing job's
+// code is kept and returned by finish().
+class Writer {
+   public:
+    Writer() : th_([this] { run(); }) {}
+    ~Writer() { finish(); }
+    void push(std::function<int()> job) {
+        std::lock_guard<std::mutex> lk(mu_);
+        q_.push_back(std::move(job));
+        cv_.notify_one();
+    }
+    // block until fewer than n jobs are queued or running
+    void wait_below(size_t n) {
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return q_.size() + busy_ < n; });
+    }
+    int finish() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_one();
+        if (th_.joinable()) th_.join();
+        return err_;
+    }
+
+   private:
+    void run() {
+        for (;;) {
+            std::function<int()> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;
+                job = std::move(q_.front());
+                q_.pop_front();
+                busy_ = 1;
+            }
+            const int rc = job();
+            std::lock_guard<std::mutex> lk(mu_);
+            if (rc && !err_) err_ = rc;
+            busy_ = 0;
+            done_.notify_all();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    std::deque<std::function<int()>> q_;
+    size_t busy_ = 0;
+    bool stop_ = false;
+    int err_ = 0;
+    std::thread th_;
+};
 
 }  // namespace
 
@@ -157,6 +222,23 @@ int main(int argc, char** argv) {
 
     int iframe = 0, iframe2d = 0;
     double t_io = 0.0;
+    Writer writer;
+    // two sets of frame buffers, used in turn; the writer runs its jobs in
+    // order, so a set is free once at most the previous stamp's jobs are left
+    // page-locked (tslb_host_alloc), so the downloads run at the full PCIe rate
+    struct FrameBuf {
+        float* f[4] = {nullptr, nullptr, nullptr, nullptr};   // phi, u, v, w
+        ~FrameBuf() {
+            for (float* p : f) tslb_host_free(p);
+        }
+        bool ensure(int k, long long n) {
+            if (!f[k]) f[k] = static_cast<float*>(tslb_host_alloc((long long)sizeof(float) * n));
+            return f[k] != nullptr;
+        }
+    };
+    std::shared_ptr<FrameBuf> bufs[2] = {std::make_shared<FrameBuf>(), std::make_shared<FrameBuf>()};
+    int ibuf = 0;
+    size_t last_jobs = 0;
     const long long step0 = tslb_steps_done(ctx);
     const double t1 = now();
     for (int s = 1; s <= o.steps; ++s) {
@@ -172,32 +254,61 @@ int main(int argc, char** argv) {
         const bool slice = o.stamp2d > 0 && step % o.stamp2d == 0;
         const bool dump = o.dump > 0 && step % o.dump == 0;
         if (!(frame || slice || dump)) continue;
+        // the steps queued so far are stepping time, not output time
+        if (check(ctx, tslb_synchronize(ctx), "tslb_synchronize")) return 1;
         const double ti = now();
+        char path[4096];
         if (frame || slice) {
-            if (check(ctx, tslb_download_moments(ctx, F[RHO].data(), F[U].data(), F[V].data(), F[W].data(), nullptr,
-                                                 nullptr, nullptr, nullptr, nullptr, nullptr, F[PHI].data()),
+            // fields of this frame in a buffer set of their own, written by the writer thread
+            writer.wait_below(last_jobs + 1);
+            std::shared_ptr<FrameBuf> fb = bufs[ibuf];
+            ibuf ^= 1;
+            size_t jobs = 0;
+            for (int k = 0; k < (slice ? 4 : 1); ++k)
+                if (!fb->ensure(k, n)) {
+                    std::fprintf(stderr, "tslb_run: page-locked frame buffer allocation failed\n");
+                    return 1;
+                }
+            if (check(ctx, tslb_download_moments(ctx, nullptr, slice ? fb->f[1] : nullptr, slice ? fb->f[2] : nullptr,
+                                                 slice ? fb->f[3] : nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                 nullptr, nullptr, fb->f[0]),
                       "tslb_download_moments"))
                 return 1;
-        }
-        char path[4096];
-        if (frame) {
-            ++iframe;
-            double red[TSLB_NREDUCE];
-            if (check(ctx, tslb_reduce(ctx, red), "tslb_reduce")) return 1;
-            if (!o.quiet)
-                std::printf("step : %8lld  mass %.9e  mass_a %.9e  mom_z %.6e  umax %.6e\n", step,
-                            red[TSLB_RED_MASS], red[TSLB_RED_MASS_A], red[TSLB_RED_MOM_Z], red[TSLB_RED_UMAX]);
-            tslb_frame_path(path, sizeof(path), o.out.c_str(), "out", "phi", iframe, "vti");
-            if (check(ctx, tslb_write_vti(path, "phi", nx, ny, nz, 1, F[PHI].data()), "tslb_write_vti")) return 1;
-        }
-        if (slice) {
-            ++iframe2d;
-            const char* names[4] = {"phi", "u", "v", "w"};
-            const int idx[4] = {PHI, U, V, W};
-            for (int k = 0; k < 4; ++k)
-                if (check(ctx, tslb_write_slices(o.out.c_str(), names[k], iframe2d, nx, ny, nz, F[idx[k]].data()),
-                          "tslb_write_slices"))
-                    return 1;
+            if (frame) {
+                ++iframe;
+                double red[TSLB_NREDUCE];
+                if (check(ctx, tslb_reduce(ctx, red), "tslb_reduce")) return 1;
+                if (!o.quiet)
+                    std::printf("step : %8lld  mass %.9e  mass_a %.9e  mom_z %.6e  umax %.6e\n", step,
+                                red[TSLB_RED_MASS], red[TSLB_RED_MASS_A], red[TSLB_RED_MOM_Z], red[TSLB_RED_UMAX]);
+                tslb_frame_path(path, sizeof(path), o.out.c_str(), "out", "phi", iframe, "vti");
+                const std::string vti(path);
+                ++jobs;
+                writer.push([vti, fb, nx, ny, nz] {
+                    const int rc = tslb_write_vti(vti.c_str(), "phi", nx, ny, nz, 1, fb->f[0]);
+                    if (rc) std::fprintf(stderr, "tslb_run: writing %s failed (%d)\n", vti.c_str(), rc);
+                    return rc;
+                });
+            }
+            if (slice) {
+                ++iframe2d;
+                const std::string dir = o.out;
+                const int k2 = iframe2d;
+                ++jobs;
+                writer.push([dir, k2, fb, nx, ny, nz] {
+                    const char* names[4] = {"phi", "u", "v", "w"};
+                    const float* data[4] = {fb->f[0], fb->f[1], fb->f[2], fb->f[3]};
+                    for (int k = 0; k < 4; ++k) {
+                        const int rc = tslb_write_slices(dir.c_str(), names[k], k2, nx, ny, nz, data[k]);
+                        if (rc) {
+                            std::fprintf(stderr, "tslb_run: writing the %s slices failed (%d)\n", names[k], rc);
+                            return rc;
+                        }
+                    }
+                    return 0;
+                });
+            }
+            last_jobs = jobs;
         }
         if (dump) {
             tslb_frame_path(path, sizeof(path), o.out.c_str(), "dump", "state", (int)step, "ckpt");
@@ -207,6 +318,7 @@ int main(int argc, char** argv) {
         t_io += now() - ti;
     }
     if (check(ctx, tslb_synchronize(ctx), "tslb_synchronize")) return 1;
+    if (writer.finish()) return 1;
     const double t2 = now();
     const double wall = t2 - t1;
     std::printf("glups: %.6f\n", (double)n * o.steps / 1e9 / wall);

@@ -51,6 +51,14 @@ int tslb_checkpoint_load(tslb_ctx* ctx, const char* path);
  * loaded checkpoint's save). */
 long long tslb_steps_done(tslb_ctx* ctx);
 
+/* Page-locked host memory for the upload and download arrays of a host that
+ * does not call the CUDA runtime itself (a Fortran driver, tslb_run): copies
+ * from and to it run at the full PCIe rate without a staging copy.  No
+ * counterpart in the reference, whose arrays are plain Fortran allocations.
+ * tslb_host_alloc returns NULL on failure; tslb_host_free(NULL) does nothing. */
+void* tslb_host_alloc(long long bytes);
+void  tslb_host_free(void* p);
+
 #ifdef __cplusplus
 }
 #endif

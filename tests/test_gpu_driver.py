@@ -85,3 +85,28 @@ def test_driver_jet_restarts_from_its_dump(tmp_path):
     restarted = read_vti_data(b / "out_phi_000001.vti")
     assert np.array_equal(full, restarted)
     assert (full > 0).sum() > 0  # the jet has entered
+
+
+def test_host_alloc_buffers_take_downloads():
+    """tslb_host_alloc gives page-locked memory that downloads fill like any
+    host array (the C++ driver downloads its frames into it)."""
+    import ctypes
+    L = capi.lib()
+    p, f = workloads.droplet(n=24, radius=6.0)
+    n = 24 ** 3
+    assert not L.tslb_host_alloc(0)
+    ptr = L.tslb_host_alloc(4 * n)
+    assert ptr
+    try:
+        buf = np.ctypeslib.as_array((ctypes.c_float * n).from_address(ptr))
+        with Lattice(p, 24, 24, 24) as lat:
+            lat.upload_moments(f)
+            lat.step(5)
+            ref = lat.download()
+            null = ctypes.POINTER(ctypes.c_float)()
+            args = [null] * 10 + [ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float))]
+            assert L.tslb_download_moments(lat.h, *args) == capi.OK
+        assert np.array_equal(buf.reshape(24, 24, 24), ref["phi"])
+    finally:
+        L.tslb_host_free(ptr)
+    L.tslb_host_free(None)
