@@ -604,9 +604,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         cp_async_commit();
         if (more) stage_mom(s + 1);
         cp_async_commit();
-        cp_async_wait<2>();  // this thread's moment copies of plane s have landed
-        // VEC staging lets threads copy other threads' nodes: make the copies visible
-        if (VEC) __syncthreads();
+        // non-VEC: this thread's own moment copies of plane s; VEC: every copy of
+        // plane s was waited for before the previous plane's pre-pull barrier
+        if (!VEC) cp_async_wait<2>();
         // ---- 1. coefficients of source plane s: own column and one rim node ----
         bool zsolid;
         const int gz = zwrap(s, zsolid);
@@ -648,7 +648,10 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
             coef_node(cn0, ci0, mi0, pi0);
             if (has_rim) coef_node(cn1, ci1, mi1, pi1);
         }
-        cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
+        // VEC: all copies issued so far (moments of s+1, phi of s+2) land before the
+        // barrier, which also makes them visible for the next plane's coefficients
+        if (VEC) cp_async_wait<0>();
+        else cp_async_wait<1>();  // this thread's phi copies of plane s+2 have landed
         __syncthreads();
         // ---- 2. pull ----
         if (active) {
