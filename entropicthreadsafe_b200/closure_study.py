@@ -4,7 +4,7 @@ vs fine plain).
     python -m entropicthreadsafe_b200.closure_study [--out result.json] [--shrink K]
 
 1. Fine plain runs (384 x 384 x 768, three inlet-noise seeds) are the
-   judge: their time-averaged fields, averaged over the seeds, give the
+   reference: their time-averaged fields, averaged over the seeds, give the
    reference jet statistics, and the spread over the seeds is the noise
    floor of one realisation.  Snapshots of two of them, box-filtered onto
    the coarse grid (tslb_closure_dataset_add_fine), are the training set;

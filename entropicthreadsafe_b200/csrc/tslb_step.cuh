@@ -17,6 +17,9 @@
 //      supplied at the target from its own node (bounce-back, regularized
 //      velocity faces);
 //   4. target plane s-1 is complete: its 11 moments are written out.
+// One CTA barrier per plane, between 1 and 2: before it every thread waits
+// for its own copies of step 0, so the barrier publishes the coefficients of
+// plane s and the staged data of plane s+1 alike.
 // Reading moments and writing moments is all the HBM traffic there is:
 // the populations f, g of the reference (recursive_2c_TSLB3D.f90:54) never
 // exist in memory.
@@ -408,10 +411,6 @@ __device__ __forceinline__ XYNode xy_node(const StepArgs& a, int gx, int gy, boo
 __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async16(float* sdst, const float* gsrc) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async16s(unsigned sa, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");

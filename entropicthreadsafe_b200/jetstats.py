@@ -76,16 +76,16 @@ def jet_statistics(mean_w: np.ndarray, mean_phi: np.ndarray, cx: float, cy: floa
     return out
 
 
-def compare(stats: dict, judge: dict) -> dict:
-    """Relative differences of the scalar statistics and profiles against the judge run."""
+def compare(stats: dict, ref: dict) -> dict:
+    """Relative differences of the scalar statistics and profiles against the reference (fine-grid) run."""
     res = {}
     for k in ("spreading_rate", "decay_rate", "mixing_thickness", "centreline_mean"):
-        a, b = stats[k], judge[k]
+        a, b = stats[k], ref[k]
         res[k] = float(abs(a - b) / abs(b)) if np.isfinite(a) and np.isfinite(b) and b != 0 else float("nan")
-    z0, z1 = judge["window"]
-    sel = (judge["z"] >= z0) & (judge["z"] <= z1)
+    z0, z1 = ref["window"]
+    sel = (ref["z"] >= z0) & (ref["z"] <= z1)
     for k in ("wc", "r_half", "delta"):
-        a, b = np.asarray(stats[k])[sel], np.asarray(judge[k])[sel]
+        a, b = np.asarray(stats[k])[sel], np.asarray(ref[k])[sel]
         ok = np.isfinite(a) & np.isfinite(b)
         res[k + "_profile"] = float(np.linalg.norm(a[ok] - b[ok]) / max(np.linalg.norm(b[ok]), 1e-30)) if ok.any() else float("nan")
     return res
