@@ -216,7 +216,8 @@ def lib() -> ctypes.CDLL:
                                 ("tslb_checkpoint_load", [vp, cp], ip),
                                 ("tslb_steps_done", [vp], ctypes.c_longlong),
                                 ("tslb_host_alloc", [ctypes.c_longlong], vp),
-                                ("tslb_host_free", [vp], None)):
+                                ("tslb_host_free", [vp], None),
+                                ("tslb_release_memory", [], ip)):
             getattr(L, name).argtypes = args
             getattr(L, name).restype = res
         _lib = L

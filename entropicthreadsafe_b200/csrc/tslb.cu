@@ -483,8 +483,10 @@ cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
 // come from one memory pool per device that keeps freed memory for the next
 // lattice: a lattice created after another was destroyed reuses its pages
 // instead of mapping new ones.  Allocation and release are ordered on the
-// lattice's stream.  A failed allocation first returns the pool's cached
-// memory to the device and is tried once more.
+// lattice's stream.  The pool keeps at most 1/8 of the device's memory
+// cached (the excess goes back at synchronisation points); a failed
+// allocation first returns all cached memory and is tried once more, and
+// tslb_release_memory returns it on request.
 std::mutex g_pool_mu;
 constexpr int MAX_DEVICES = 64;
 cudaMemPool_t g_pool[MAX_DEVICES] = {};
@@ -502,7 +504,9 @@ cudaError_t pool_alloc(void** ptr, size_t bytes, int dev, cudaStream_t st) {
             props.location.id = dev;
             cudaError_t e = cudaMemPoolCreate(&pool, &props);
             if (e != cudaSuccess) return e;
-            unsigned long long keep = ~0ULL;
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            unsigned long long keep = (unsigned long long)total_b / 8;
             e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
             if (e != cudaSuccess) {
                 cudaMemPoolDestroy(pool);
@@ -1168,6 +1172,13 @@ int tslb_synchronize(tslb_ctx* c) {
 }
 
 void* tslb_stream(tslb_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int tslb_release_memory(void) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (int d = 0; d < MAX_DEVICES; ++d)
+        if (g_pool[d] && cudaMemPoolTrimTo(g_pool[d], 0) != cudaSuccess) return TSLB_ERR_CUDA;
+    return TSLB_OK;
+}
 
 long long tslb_launch_count(tslb_ctx* c) { return c ? c->launches : 0; }
 

@@ -255,6 +255,12 @@ int  tslb_synchronize(tslb_ctx* ctx);
  * CUDA events against the step. */
 void* tslb_stream(tslb_ctx* ctx);
 
+/* Device memory of destroyed lattices stays cached for the next lattice (up
+ * to 1/8 of each device's memory); this returns all of it to the devices,
+ * e.g. before the host allocates large buffers of its own.  No counterpart
+ * in the reference, which allocates its arrays once. */
+int tslb_release_memory(void);
+
 /* Number of kernel launches the context has issued since creation. */
 long long tslb_launch_count(tslb_ctx* ctx);
 

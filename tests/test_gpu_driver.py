@@ -110,3 +110,24 @@ def test_host_alloc_buffers_take_downloads():
     finally:
         L.tslb_host_free(ptr)
     L.tslb_host_free(None)
+
+
+def test_release_memory_returns_the_cached_lattice_memory():
+    """A destroyed lattice's device memory stays cached for the next lattice;
+    tslb_release_memory gives it back to the device."""
+    import torch
+    L = capi.lib()
+    p, f = workloads.droplet(n=96, radius=20.0)
+    with Lattice(p, 96, 96, 96) as lat:   # two 11-field states of 96^3 nodes: 78 MB
+        lat.upload_moments(f)
+        lat.step(1)
+    torch.cuda.synchronize()
+    free_cached, _ = torch.cuda.mem_get_info()
+    assert L.tslb_release_memory() == capi.OK
+    free_released, _ = torch.cuda.mem_get_info()
+    assert free_released - free_cached >= 60e6
+    # lattices still work after the release
+    with Lattice(p, 96, 96, 96) as lat:
+        lat.upload_moments(f)
+        lat.step(1)
+        assert abs(lat.reduce()["mass"] - f["rho"].astype(np.float64).sum()) < 1e-3 * 96 ** 3
