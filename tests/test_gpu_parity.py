@@ -252,6 +252,43 @@ def test_uniform_colour_is_kept_exactly():
     assert np.all(gpu["phi"] == -1.0)
 
 
+@pytest.mark.parametrize("walls", ["periodic", "bounceback_z", "moving_wall_z"])
+def test_single_colour_kernel_matches_pinned_phase_field_oracle(walls):
+    """The colour kernel with one colour everywhere, no force and equal
+    relaxation times against the phase-field oracle at sigma = 0, whose f
+    step is the reference's fused_TSLB_1c pinned by the golden vectors: the
+    colour kernel's equilibrium, regularization, streaming and walls."""
+    nx, ny, nz = 40, 12, 10
+    bc = [capi.BC_PERIODIC] * 6
+    bcu = [[0.0, 0.0, 0.0]] * 6
+    if walls != "periodic":
+        bc[capi.FACE_ZM] = capi.BC_BOUNCEBACK
+        bc[capi.FACE_ZP] = capi.BC_BOUNCEBACK if walls == "bounceback_z" else capi.BC_VELOCITY
+        if walls == "moving_wall_z":
+            bcu = [[0.0, 0.0, 0.0]] * 5 + [[0.03, 0.0, 0.0]]
+    rng = np.random.default_rng(7)
+    f = workloads.empty_fields(nx, ny, nz)
+    for k in ("u", "v", "w"):
+        f[k][:] = rng.normal(0, 0.02, f[k].shape)
+    for k in ("pxx", "pxy", "pxz", "pyy", "pyz", "pzz"):
+        f[k][:] = rng.normal(0, 1e-4, f[k].shape)
+    f["rho"][:] = 1.0 + rng.normal(0, 1e-3, f["rho"].shape)
+    f["phi"][:] = 1.0
+    pc = capi.make_params(mode=capi.MODE_COLOUR, tau_a=0.7, tau_b=0.7, sigma=0.01, beta=0.7, bc=bc, bc_u=bcu,
+                          bc_phi=[1.0] * 6, wall_phi_mode=1)
+    pp = capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=0.7, sigma=0.0, bc=bc, bc_u=bcu, bc_phi=[1.0] * 6)
+    gpu, _ = run_gpu(pc, f, 40)
+    o64, _ = run_oracle(pp, f, 40, fp64=True)
+    o32, _ = run_oracle(pp, f, 40, fp64=False)
+    assert np.all(gpu["phi"] == 1.0)
+    for d in (gpu, o64, o32):
+        d.pop("phi")
+    eg = {k: rel_err(gpu[k], o64[k]) for k in gpu}
+    e32 = {k: rel_err(o32[k], o64[k]) for k in gpu}
+    bad = {k: (eg[k], e32[k]) for k in eg if eg[k] > max(TARGET, TOL_FACTOR * e32[k])}
+    assert not bad, (walls, bad)
+
+
 def test_colour_droplet_bounceback_all_faces():
     """Walls on x, y and z faces (lateral solid sources and solid planes)."""
     p, f = workloads.droplet(n=20, radius=5.0, tau=0.9, sigma=0.01, beta=0.7)
