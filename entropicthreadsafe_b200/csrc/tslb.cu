@@ -103,6 +103,8 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
     a.dtau = c->closure ? c->dtau : (c->base_on ? c->dtau_base : nullptr);
     a.solid = c->solid_on ? c->solid : nullptr;
     a.near = c->solid_on ? c->near : nullptr;
+    a.sr = 1;
+    a.sr_step = (unsigned int)c->steps_done;
     for (int f = 0; f < NF; ++f) {
         a.scale[f] = c->scale[f];
         a.iscale[f] = 1.0f / c->scale[f];
@@ -1424,6 +1426,9 @@ int ens_build(tslb_ensemble* e) {
         for (int par = 0; par < 2; ++par) {
             const int cur = c->cur ^ par;
             args[par].push_back(make_args(c, c->state[cur], c->state[cur ^ 1]));
+            // the ensemble replays these arguments every step (CUDA graph): no step
+            // counter to seed stochastic rounding, so 16-bit members round to nearest
+            args[par].back().sr = 0;
         }
     }
     ens_drop_graph(e);

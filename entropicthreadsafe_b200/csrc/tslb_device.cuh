@@ -93,6 +93,8 @@ struct StepArgs {
     const float* dtau;      // colour: per-node correction of tau (stride N), or null
     const unsigned int* solid;  // interior solid nodes, one bit per node (bit i & 31 of word i >> 5), or null
     const unsigned int* near;   // fluid nodes with a solid one among their 26 neighbours, same layout
+    int sr;                 // 16-bit storage: store the moments with stochastic rounding
+    unsigned int sr_step;   // step counter that seeds the rounding (with the node and the field)
 };
 
 // Counter-based uniform in [0, 1) of four integers: the reference's
@@ -186,6 +188,55 @@ template <class T>
 __device__ __forceinline__ T cvt_out(float v, const StepArgs& a, int f) {
     if constexpr (std::is_same<T, __half>::value) return Stor<T>::st(v * a.scale[f]);
     else return Stor<T>::st(v);
+}
+
+// Stochastic rounding of the 16-bit stored moments: a value rounds away from
+// zero with the probability of its distance from the value toward zero, so
+// the expected stored value is the FP32 one.  Rounding to nearest drops every
+// change smaller than half a unit in the last place at every step - the body
+// force of the channel adds about 2.5e-6 to u per step, 1/200 of a BF16 unit
+// at u = 0.07 - and the stored flow stops following the forcing.  The random
+// bits hash the node, the field and the step counter, so a run (and its
+// restart from a checkpoint) is reproducible.
+__device__ __forceinline__ unsigned int sr_node(unsigned int node, unsigned int step) {
+    unsigned int h = node * 0x9E3779B1u ^ (step * 0x85EBCA77u + 0x165667B1u);
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h;
+}
+__device__ __forceinline__ unsigned int sr_field(unsigned int hnode, int f) {
+    unsigned int h = (hnode + (unsigned int)f * 0x9E3779B9u) * 0x85EBCA6Bu;
+    return h ^ (h >> 16);
+}
+// BF16: add 16 random bits below the kept mantissa, then truncate (the sign
+// stays, so magnitudes round up); non-finite values pass unchanged
+__device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned int r) {
+    unsigned int b = __float_as_uint(v);
+    if ((b & 0x7F800000u) != 0x7F800000u) b += r & 0xFFFFu;
+    return __ushort_as_bfloat16((unsigned short)(b >> 16));
+}
+// FP16 (of the scaled value x): toward zero, then one unit away from zero with
+// probability |x - lo| / ulp; never up to infinity
+__device__ __forceinline__ __half f16_sr(float x, unsigned int r) {
+    const __half lo = __float2half_rz(x);
+    const float lof = __half2float(lo);
+    const float res = fabsf(x - lof);
+    if (!(res > 0.f) || !isfinite(x)) return lo;
+    const unsigned short hb = __half_as_ushort(lo);
+    const unsigned short nb =
+        (hb & 0x7FFFu) == 0 ? (unsigned short)((x < 0.f ? 0x8000u : 0u) | 1u) : (unsigned short)(hb + 1u);
+    if ((nb & 0x7C00u) == 0x7C00u) return lo;
+    const __half hi = __ushort_as_half(nb);
+    const float ulp = fabsf(__half2float(hi) - lof);
+    const float u01 = (float)(r >> 8) * (1.0f / 16777216.0f);
+    return u01 * ulp < res ? hi : lo;
+}
+template <class T>
+__device__ __forceinline__ T cvt_out_sr(float v, const StepArgs& a, int f, unsigned int r) {
+    if constexpr (std::is_same<T, __half>::value) return f16_sr(v * a.scale[f], r);
+    else if constexpr (std::is_same<T, __nv_bfloat16>::value) return bf16_sr(v, r);
+    else return v;
 }
 template <class T>
 __device__ __forceinline__ float ld_field(const StepArgs& a, int f, long long idx) {

@@ -703,9 +703,11 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 float chk = 0.f;
                 // single-component mode does not step phi (held at 1 in both buffers)
                 constexpr int nout = MODE == TSLB_MODE_SINGLE ? F_PHI : NF;
+                // 16-bit storage: stochastic rounding seeded by the node and the step
+                const unsigned int hnode = sizeof(T) == 2 ? sr_node((unsigned int)(t * plane + cn0.off), a.sr_step) : 0u;
 #pragma unroll
                 for (int f = 0; f < nout; ++f) {
-                    const T st = cvt_out<T>(o[f], a, f);
+                    const T st = (sizeof(T) == 2 && a.sr) ? cvt_out_sr<T>(o[f], a, f, sr_field(hnode, f)) : cvt_out<T>(o[f], a, f);
                     po[f * a.N] = st;
                     chk += Stor<T>::ld(st);
                 }
