@@ -216,21 +216,13 @@ __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned int r) {
     if ((b & 0x7F800000u) != 0x7F800000u) b += r & 0xFFFFu;
     return __ushort_as_bfloat16((unsigned short)(b >> 16));
 }
-// FP16 (of the scaled value x): toward zero, then one unit away from zero with
-// probability |x - lo| / ulp; never up to infinity
+// FP16 (of the scaled value x): the hardware's stochastically rounded
+// conversion (cvt.rs, sm_100a) with the random bits r; the value fills both
+// halves and the low half is kept
 __device__ __forceinline__ __half f16_sr(float x, unsigned int r) {
-    const __half lo = __float2half_rz(x);
-    const float lof = __half2float(lo);
-    const float res = fabsf(x - lof);
-    if (!(res > 0.f) || !isfinite(x)) return lo;
-    const unsigned short hb = __half_as_ushort(lo);
-    const unsigned short nb =
-        (hb & 0x7FFFu) == 0 ? (unsigned short)((x < 0.f ? 0x8000u : 0u) | 1u) : (unsigned short)(hb + 1u);
-    if ((nb & 0x7C00u) == 0x7C00u) return lo;
-    const __half hi = __ushort_as_half(nb);
-    const float ulp = fabsf(__half2float(hi) - lof);
-    const float u01 = (float)(r >> 8) * (1.0f / 16777216.0f);
-    return u01 * ulp < res ? hi : lo;
+    unsigned int d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(x), "r"(r));
+    return __ushort_as_half((unsigned short)(d & 0xFFFFu));
 }
 template <class T>
 __device__ __forceinline__ T cvt_out_sr(float v, const StepArgs& a, int f, unsigned int r) {
