@@ -1,0 +1,30 @@
+"""The ctypes mirror of tslb_params has the C layout of include/tslb.h, field
+by field (a C program compiled here prints the offsets; CPU only)."""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from entropicthreadsafe_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs a C compiler")
+def test_params_field_offsets_match_the_header(tmp_path):
+    names = [f[0] for f in capi.TslbParams._fields_]
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "tslb.h"', "int main(void) {",
+             '  printf("sizeof %zu\\n", sizeof(tslb_params));']
+    lines += [f'  printf("{n} %zu\\n", offsetof(tslb_params, {n}));' for n in names]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    assert int(out["sizeof"]) == ctypes.sizeof(capi.TslbParams)
+    for n in names:
+        assert int(out[n]) == getattr(capi.TslbParams, n).offset, n
