@@ -28,3 +28,13 @@ def test_params_field_offsets_match_the_header(tmp_path):
     assert int(out["sizeof"]) == ctypes.sizeof(capi.TslbParams)
     for n in names:
         assert int(out[n]) == getattr(capi.TslbParams, n).offset, n
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs a C compiler")
+def test_headers_compile_as_c99(tmp_path):
+    """A C host includes the three public headers without a C++ compiler."""
+    src = tmp_path / "hosts.c"
+    src.write_text('#include "tslb.h"\n#include "tslb_io.h"\n#include "tslb_closure.h"\n'
+                   "int main(void) { tslb_params p; tslb_default_params(&p); return p.mode; }\n")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"), "-c",
+                    "-o", str(tmp_path / "hosts.o"), str(src)], check=True)
