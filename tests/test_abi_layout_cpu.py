@@ -38,3 +38,29 @@ def test_headers_compile_as_c99(tmp_path):
                    "int main(void) { tslb_params p; tslb_default_params(&p); return p.mode; }\n")
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"), "-c",
                     "-o", str(tmp_path / "hosts.o"), str(src)], check=True)
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs a C compiler")
+def test_c_host_links_and_gets_an_error_code_not_an_abort(tmp_path):
+    """A C program links against libtslb.so and calls tslb_create: on a machine
+    without a GPU it gets an error code and a message, the process lives on."""
+    capi.lib()   # built in-tree
+    lib_dir = os.path.dirname(capi.LIB_PATH)
+    src = tmp_path / "host.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "tslb.h"\n'
+        "int main(void) {\n"
+        "  tslb_params p; tslb_default_params(&p);\n"
+        "  tslb_ctx* c = NULL;\n"
+        "  int rc = tslb_create(&p, 16, 16, 16, &c);\n"
+        '  if (rc == TSLB_OK) { tslb_destroy(c); printf("created\\n"); return 0; }\n'
+        '  printf("error %d %s\\n", rc, tslb_last_error(NULL));\n'
+        "  return c == NULL ? 0 : 1;\n"
+        "}\n")
+    exe = tmp_path / "host"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src),
+                    "-L" + lib_dir, "-ltslb", "-Wl,-rpath," + lib_dir], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = r.stdout.strip()
+    assert out == "created" or (out.startswith("error ") and len(out.split(" ", 2)[2]) > 0), out
