@@ -447,7 +447,8 @@ def run_ours(args):
             lp.synchronize()
             ms_p = e0.elapsed_time(e1) / args.steps
             forms[name] = {"value": ws * nodes / (ms_p * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_p,
-                           "speedup_vs_fp32": ms_step / ms_p, "bytes_per_lu": 44}
+                           "speedup_vs_fp32": ms_step / ms_p, "bytes_per_lu": 44,
+                           "rounding": "stochastic (hashed from node, field and step)"}
             lp.close()
         p.precision = capi.PREC_FP32
     ens = None if args.no_ensemble else ensemble_leg(args)
