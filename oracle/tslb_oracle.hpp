@@ -461,9 +461,22 @@ struct Oracle {
         return n;
     }
 
+    // in-plane coordinate of the ghost node a population comes from: periodic
+    // axes wrap, a non-periodic axis clamps to the lattice
+    int src_coord(int axis, int c) const {
+        const int n = dim(axis);
+        if (c >= 0 && c < n) return c;
+        if (periodic(axis)) return (c % n + n) % n;
+        return c < 0 ? 0 : n - 1;
+    }
+
     // Regularized population entering fluid node (i,j,k) from a velocity
     // face in direction q: f^eq(rho_x, U_b) + (1-omega) w a^neq(Pi_x, u_x)
-    // (boundary_cds_3D_module.f90:454-629, 931-1048).
+    // (boundary_cds_3D_module.f90:454-629, 931-1048).  U_b is the velocity of
+    // the ghost node the population leaves, (i,j,k) - c_q: the inlet plane at
+    // that node's in-plane position (:934, w(i,j,k) of the ghost node i,j,1),
+    // and for the outlet the normal velocity of the fluid node next to it
+    // (:992, w(i,j,nz) = w(i,j,nz-1)).
     void velocity_face_value(int fc, int q, int i, int j, int k) {
         size_t x = id(i, j, k);
         const R rho = M[RHO][x], u = M[UX][x], v = M[UY][x], w = M[UZ][x];
@@ -473,17 +486,22 @@ struct Oracle {
         const int axis = fc / 2;
         R Ub[3] = {R(prm.bc_u[fc][0]), R(prm.bc_u[fc][1]), R(prm.bc_u[fc][2])};
         R phib = prm.bc_phi[fc] < -2.0f ? phi : R(prm.bc_phi[fc]);
-        const R uvw[3] = {u, v, w};
+        // the ghost node's in-plane position; the layer coordinate stays the target's
+        int g[3] = {i, j, k};
+        const int cq[3] = {CX[q], CY[q], CZ[q]};
+        for (int a = 0; a < 3; ++a)
+            if (a != axis) g[a] = src_coord(a, g[a] - cq[a]);
         if (bc == TSLB_BC_INLET) {
-            for (int a = 0; a < 3; ++a) Ub[a] = inlet_val(fc, a, i, j, k);
-            phib = inlet_val(fc, 3, i, j, k);
+            for (int a = 0; a < 3; ++a) Ub[a] = inlet_val(fc, a, g[0], g[1], g[2]);
+            phib = inlet_val(fc, 3, g[0], g[1], g[2]);
         } else if (bc == TSLB_BC_OUTLET) {
-            Ub[axis] = uvw[axis];
+            Ub[axis] = M[UX + axis][id(g[0], g[1], g[2])];
             phib = phi;
         }
         R rho_b = rho;
         if (bc == TSLB_BC_PRESSURE) {
             // pressure outlet (no reference counterpart): density 1, the node's velocity and phi
+            const R uvw[3] = {u, v, w};
             for (int a = 0; a < 3; ++a) Ub[a] = uvw[a];
             phib = phi;
             rho_b = R(1);

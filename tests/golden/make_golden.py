@@ -15,6 +15,9 @@ evaluation equals the serial loop):
   collision with force TSLB_2C-mpi/lb_kernels_module.f90:747-931
   bounce-back          boundary_cds_3D_module.f90:18-70
   moving walls         boundary_cds_3D_module.f90:413-571
+  jet walls, inlet and boundary_cds_3D_module.f90:885-1050 (bcs_2c_turbulent_jet:
+  outlet               bounce-back of the solid planes, regularized inlet at
+                       k = 1, zero-gradient outlet at k = nz)
 
 Translation is mechanical: array references `a(i+1,j,k-1,q)` become
 shifted numpy views, `x_db` literals drop the kind suffix, `if` blocks
@@ -24,11 +27,23 @@ exchange (phi, normals, moments), applied before and after the wall
 conditions.  FP32 runs hold every variable in float32 (the reference's
 db=4 build); FP64 runs hold every variable in float64.
 
-Output: tests/golden/<case>.npz with the interior populations after the
-initial conditions (the oracle's input), the parameters, and the moment
-fields after `nsteps` steps (the golden output).  Run from the repo root:
+The jet case stands a fixed inlet plane in for the host random_number
+refresh of the inlet velocity (:866-877, compiler-defined): u = v = 0 and a
+Gaussian w profile on the k = 1 plane, phi = 1 on a disc; the solid planes'
+moments are never touched by the moments pass (it skips isfluid = 0 nodes),
+so the plane stays as set, and the outlet plane's tangential velocity stays
+at its initial 0.  The only rewrite of the source text: inside the
+`elseif(k.eq.nz)` branch the index `nz-1` is the offset k-1.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+Output: tests/golden/<case>.npz with the interior populations after the
+initial conditions (the oracle's input) -- or, for the 32^3 case, the
+FP32-representable initial moments (f = f^eq, so uploading them with
+Pi^neq = 0 is the same state) --, the parameters, and the moment fields
+after `nsteps` steps (the golden output; the 32^3 case keeps the FP64
+result rounded to FP32 and the per-field spread of the FP32 run).  Run from
+the repo root, with the reference checkout's path:
+
+    python tests/golden/make_golden.py --reference <path to entropicThreadsafe>
 """
 from __future__ import annotations
 
@@ -52,6 +67,7 @@ BLOCKS = {
     "collision_force": ("TSLB_2C-mpi/lb_kernels_module.f90", 747, 931),
     "bounceback": ("boundary_cds_3D_module.f90", 18, 70),
     "couette": ("boundary_cds_3D_module.f90", 413, 571),
+    "jet": ("boundary_cds_3D_module.f90", 885, 1050),
 }
 
 
@@ -109,6 +125,9 @@ def _offset(arg: str, var: str) -> int:
     arg = arg.replace(" ", "")
     if arg == var:
         return 0
+    if var == "k" and arg == "nz-1":
+        # only inside the jet outlet branch `elseif(k.eq.nz)` (checked in run_case)
+        return -1
     m = re.fullmatch(var + r"([+-]\d+)", arg)
     if not m:
         raise ValueError(f"unsupported index {arg!r}")
@@ -253,6 +272,15 @@ CASES = {
     "couette": dict(n=(6, 6, 8), walls="couette", collision="collision", nsteps=12,
                     tau=0.625, sigma=0.0, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.046875,
                     droplet=None, urand=0.005, seed=13),
+    # x,y periodic, jet walls: fixed inlet plane at k = 1, zero-gradient outlet at k = nz
+    "pf_jet": dict(n=(8, 8, 10), walls="jet", collision="collision", nsteps=12,
+                   tau=0.75, sigma=0.01, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.0,
+                   droplet=None, urand=0.005, seed=14,
+                   inlet=dict(centre=(4.5, 4.5), w=0.05, width=2.0, radius=2.5)),
+    # fully periodic 32^3 droplet, 100 steps (initial moments stored, not populations)
+    "pf_droplet32": dict(n=(32, 32, 32), walls=None, collision="collision", nsteps=100,
+                         tau=0.8, sigma=0.01, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.0,
+                         droplet=(16.5, 16.5, 16.5, 8.0), urand=0.002, seed=15, moments_only=True),
 }
 
 
@@ -274,8 +302,22 @@ def run_case(ref: str, cfg: dict, dtype):
         cx, cy, cz, R = cfg["droplet"]
         r = np.sqrt((i - cx) ** 2 + (j - cy) ** 2 + (k - cz) ** 2)
         phi = 0.5 * (1 + np.tanh((R - r) / 1.0))
+    ic = {}
     for name, val in (("rho", rho), ("u", uvw[0]), ("v", uvw[1]), ("w", uvw[2]), ("phi", phi)):
         G.a[name][1:-1, 1:-1, 1:-1] = np.where(fluid, val, 0.0).astype(dtype)
+    inlet = None
+    if walls == "jet":
+        # the fixed inlet plane on the solid plane k = 1 (standing in for :866-877)
+        spec = cfg["inlet"]
+        ii, jj = np.meshgrid(np.arange(1, nx + 1), np.arange(1, ny + 1), indexing="ij")
+        r2 = (ii - spec["centre"][0]) ** 2 + (jj - spec["centre"][1]) ** 2
+        w_in = (spec["w"] * np.exp(-r2 / (2 * spec["width"] ** 2))).astype(np.float32)
+        phi_in = (r2 <= spec["radius"] ** 2).astype(np.float32)
+        G.a["u"][1:-1, 1:-1, 1] = 0
+        G.a["v"][1:-1, 1:-1, 1] = 0
+        G.a["w"][1:-1, 1:-1, 1] = w_in.astype(dtype)
+        G.a["phi"][1:-1, 1:-1, 1] = phi_in.astype(dtype)
+        inlet = np.stack([np.zeros_like(w_in), np.zeros_like(w_in), w_in, phi_in])   # (4, nx, ny)
 
     t = dtype
     consts = {
@@ -287,6 +329,9 @@ def run_case(ref: str, cfg: dict, dtype):
         "uwall": t(cfg["uwall"]),
     }
     tree = {name: parse(read_block(ref, *BLOCKS[name])) for name in BLOCKS}
+    # the one rewritten index: `nz-1` of the jet block occurs in its k == nz branch only
+    jet_text = " ".join(read_block(ref, *BLOCKS["jet"])).replace(" ", "")
+    assert jet_text.count("nz-1") == 1 and jet_text.index("elseif(k.eq.nz)") < jet_text.index("nz-1")
 
     def run_block(name):
         # each block's outer `if(isfluid...)` is part of the tree
@@ -298,8 +343,24 @@ def run_case(ref: str, cfg: dict, dtype):
     f_in = G.a["f"][:, 1:nx + 1, 1:ny + 1, kz].copy()
     g_in = G.a["g"][:, 1:nx + 1, 1:ny + 1, kz].copy()
 
-    for _ in range(cfg["nsteps"]):
-        run_block("moments")
+    moments_only = cfg.get("moments_only", False)
+    if moments_only:
+        # The state a step starts from is its moments.  The first moments pass
+        # of the FP64 run (the initial populations, g written one node ahead)
+        # rounded to FP32 is the stored initial state, and both runs start
+        # from it instead of their own first moments pass.
+        if dtype == np.float64:
+            run_block("moments")
+            for name in MOMENTS:
+                ic[name] = G.a[name][1:nx + 1, 1:ny + 1, 1:nz + 1].astype(np.float32)
+            run_case.ic64 = dict(ic)
+        else:
+            ic = dict(run_case.ic64)    # the FP64 run comes first (main)
+        for name in MOMENTS:
+            G.a[name][1:nx + 1, 1:ny + 1, 1:nz + 1] = ic[name].astype(dtype)
+    for step in range(cfg["nsteps"]):
+        if step > 0 or not moments_only:
+            run_block("moments")
         G.wrap_scalar("phi")
         run_block("normals")
         for name in ("normx", "normy", "normz"):
@@ -312,10 +373,14 @@ def run_case(ref: str, cfg: dict, dtype):
             for name in MOMENTS:
                 G.wrap_scalar(name)
             run_block("couette")
+        elif walls == "jet":
+            for name in MOMENTS:
+                G.wrap_scalar(name)
+            run_block("jet")
         G.wrap_pops()
     run_block("moments")
     out = {name: G.a[name][1:nx + 1, 1:ny + 1, kz].copy() for name in MOMENTS}
-    return f_in, g_in, out
+    return f_in, g_in, out, ic, inlet
 
 
 def to_oracle_layout(a: np.ndarray) -> np.ndarray:
@@ -325,23 +390,48 @@ def to_oracle_layout(a: np.ndarray) -> np.ndarray:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TSLB_REFERENCE"),
+                    help="path of the reference checkout (or set TSLB_REFERENCE)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    ap.add_argument("--case", action="append", help="generate only these cases")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference (or TSLB_REFERENCE): the reference checkout to read the statements from")
     for name, cfg in CASES.items():
+        if args.case and name not in args.case:
+            continue
         res = {}
+        outs = {}
         for tag, dt in (("fp64", np.float64), ("fp32", np.float32)):
-            f_in, g_in, out = run_case(args.reference, cfg, dt)
+            f_in, g_in, out, ic, inlet = run_case(args.reference, cfg, dt)
+            outs[tag] = out
+            if cfg.get("moments_only"):
+                continue
             res[f"f_{tag}"] = to_oracle_layout(f_in)
             res[f"g_{tag}"] = to_oracle_layout(g_in)
             for m in MOMENTS:
                 res[f"{m}_{tag}"] = to_oracle_layout(out[m])
+        if cfg.get("moments_only"):
+            for m in MOMENTS:
+                res[f"ic_{m}"] = to_oracle_layout(ic[m])
+            for m in MOMENTS:
+                res[f"{m}_fp64"] = to_oracle_layout(outs["fp64"][m]).astype(np.float32)
+            # spread of the reference's FP32 run, max|fp32 - fp64| / max|fp64| (rho as rho - 1)
+            spread = {}
+            for m in MOMENTS:
+                a, b = outs["fp32"][m].astype(np.float64), outs["fp64"][m]
+                if m == "rho":
+                    a, b = a - 1.0, b - 1.0
+                spread[m] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+            res["fp32_spread"] = np.array(json.dumps(spread))
+        if inlet is not None:
+            res["inlet"] = np.ascontiguousarray(np.swapaxes(inlet, -1, -2))   # (4, ny, nx): u, v, w, phi of the z- face
         meta = dict(cfg)
         meta["blocks"] = {k: list(v) for k, v in BLOCKS.items()}
         res["meta"] = np.array(json.dumps(meta))
         path = os.path.join(args.out, f"{name}.npz")
         np.savez_compressed(path, **res)
-        d = max(np.abs(res[f"{m}_fp32"] - res[f"{m}_fp64"]).max() for m in MOMENTS)
+        d = max(np.abs(outs["fp32"][m] - outs["fp64"][m]).max() for m in MOMENTS)
         print(f"{name}: wrote {path} ({os.path.getsize(path)} B); max |fp32-fp64| = {d:.3e}")
 
 

@@ -9,7 +9,10 @@ import numpy as np
 from entropicthreadsafe_b200 import capi
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-GOLDEN_CASES = ("pf_periodic", "pf_walls_force", "couette")
+# golden cases given as the reference's populations after its initial conditions
+GOLDEN_CASES = ("pf_periodic", "pf_walls_force", "couette", "pf_jet")
+# the 32^3, 100-step phase-field droplet, given as its initial moments
+GOLDEN_MOMENT_CASE = "pf_droplet32"
 
 
 def golden_params(meta):
@@ -20,9 +23,25 @@ def golden_params(meta):
     elif meta["walls"] == "couette":
         bc[4] = bc[5] = capi.BC_VELOCITY
         bcu = [[0, 0, 0]] * 4 + [[-meta["uwall"], 0, 0], [meta["uwall"], 0, 0]]
+    elif meta["walls"] == "jet":
+        # bcs_2c_turbulent_jet: inlet plane at z-, zero-gradient outlet at z+ whose
+        # g6 carries phi at the fixed speed 0.05 (boundary_cds_3D_module.f90:1044-1045)
+        bc[4], bc[5] = capi.BC_INLET, capi.BC_OUTLET
+        bcu = [[0, 0, 0]] * 5 + [[0, 0, 0.05]]
     return capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=meta["tau"], sigma=meta["sigma"],
                             sharp_c=meta["sharp_c"], force=meta["force"], bc=bc, bc_u=bcu,
                             bc_phi=[0.0] * 6, wall_phi_mode=0)
+
+
+def golden_inlet(d):
+    """{face: planes} of a golden case with an inlet plane (the jet), else None."""
+    return {capi.FACE_ZM: np.asarray(d["inlet"], np.float32)} if "inlet" in d.files else None
+
+
+def golden_initial_moments(d):
+    """The 11 initial moment fields of a moments-only golden case (the first
+    moments pass of the reference's initial populations, rounded to FP32)."""
+    return {k: np.asarray(d["ic_" + k], np.float32) for k in capi.FIELDS}
 
 
 def load_golden(case):

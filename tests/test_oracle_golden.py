@@ -4,23 +4,34 @@ tests/golden/*.npz hold populations and moments produced by evaluating the
 reference's Fortran statements with numpy (tests/golden/make_golden.py):
 the phase-field step recursive_2c_TSLB3D.f90:351-832, the forced collision
 TSLB_2C-mpi/lb_kernels_module.f90:747-931, bounce-back
-boundary_cds_3D_module.f90:18-70 and the moving-wall condition
-boundary_cds_3D_module.f90:413-571.
+boundary_cds_3D_module.f90:18-70, the moving-wall condition
+boundary_cds_3D_module.f90:413-571 and the jet's inlet and outlet
+boundary_cds_3D_module.f90:885-1050 (with a fixed inlet plane).
 """
+import json
+
 import numpy as np
 import pytest
 
 import oracle
 from entropicthreadsafe_b200 import capi
 
-from helpers import GOLDEN_CASES as CASES, golden_params, load_golden as load, rel_err
+from helpers import (GOLDEN_CASES as CASES, GOLDEN_MOMENT_CASE, golden_initial_moments, golden_inlet, golden_params,
+                     load_golden as load, rel_err)
+
+
+def make_oracle(d, meta, nx, ny, nz, fp64):
+    o = oracle.Oracle(golden_params(meta), nx, ny, nz, fp64=fp64)
+    for face, planes in (golden_inlet(d) or {}).items():
+        o.set_inlet(face, planes)
+    return o
 
 
 @pytest.mark.parametrize("case", CASES)
 def test_oracle_fp64_matches_reference_statements(case):
     d, meta = load(case)
     nz, ny, nx = d["rho_fp64"].shape
-    o = oracle.Oracle(golden_params(meta), nx, ny, nz, fp64=True)
+    o = make_oracle(d, meta, nx, ny, nz, True)
     o.set_pops(d["f_fp64"], d["g_fp64"])
     o.step(meta["nsteps"])
     out = o.get_moments()
@@ -33,7 +44,7 @@ def test_oracle_fp64_matches_reference_statements(case):
 def test_oracle_fp32_matches_reference_statements(case):
     d, meta = load(case)
     nz, ny, nx = d["rho_fp32"].shape
-    o = oracle.Oracle(golden_params(meta), nx, ny, nz, fp64=False)
+    o = make_oracle(d, meta, nx, ny, nz, False)
     o.set_pops(d["f_fp32"], d["g_fp32"])
     o.step(meta["nsteps"])
     out = o.get_moments()
@@ -49,3 +60,23 @@ def test_reference_fp32_noise_is_what_the_gpu_tolerance_assumes():
     d, _ = load("pf_periodic")
     for m in capi.FIELDS:
         assert rel_err(d[m + "_fp32"], d[m + "_fp64"]) < 2e-4, m
+
+
+@pytest.mark.slow
+def test_oracle_fp64_matches_reference_statements_32cube_100_steps():
+    """The 32^3 droplet over 100 steps: the oracle from the initial moments
+    against the reference statements from their initial populations (FP64,
+    the golden rounded to FP32 when stored)."""
+    d, meta = load(GOLDEN_MOMENT_CASE)
+    nz, ny, nx = d["rho_fp64"].shape
+    o = make_oracle(d, meta, nx, ny, nz, True)
+    o.set_moments({k: v.astype(np.float64) for k, v in golden_initial_moments(d).items()})
+    o.step(meta["nsteps"])
+    out = o.get_moments()
+    for m in capi.FIELDS:
+        a, b = out[m], d[m + "_fp64"].astype(np.float64)
+        if m == "rho":
+            a, b = a - 1.0, b - 1.0
+        assert rel_err(a, b) < 1e-6, m
+    spread = json.loads(str(d["fp32_spread"]))
+    assert set(spread) == set(capi.FIELDS)
