@@ -22,6 +22,7 @@ MBC_NONE, MBC_COPY, MBC_JET = range(3)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
 NREDUCE = 12
 NOALLOC_MAX_NODES = 1 << 20
+REDUCE_QUEUE = 256
 RED_NAMES = ("mass", "mass_a", "mass_b", "mom_x", "mom_y", "mom_z", "kinetic",
              "umax", "rho_in", "rho_out", "dp", "n_in")
 FIELDS = ("rho", "u", "v", "w", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "phi")
@@ -165,6 +166,22 @@ def lib() -> ctypes.CDLL:
         L.tslb_last_error.restype = ctypes.c_char_p
         L.tslb_step_noalloc.argtypes = [vp, ip, ip, ip, vp, vp, ctypes.c_longlong, vp]
         L.tslb_step_noalloc.restype = ip
+        L.tslb_noalloc_check.argtypes = [vp]
+        L.tslb_noalloc_check.restype = ip
+        L.tslb_reduce_async.argtypes = [vp]
+        L.tslb_reduce_async.restype = ip
+        L.tslb_reduce_collect.argtypes = [vp, dp, ip, ctypes.POINTER(ctypes.c_int)]
+        L.tslb_reduce_collect.restype = ip
+        L.tslb_create_slab.argtypes = [vp, ip, ip, ip, ip, ip, ctypes.POINTER(vp)]
+        L.tslb_create_slab.restype = ip
+        L.tslb_slab_geometry.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.tslb_slab_geometry.restype = ip
+        L.tslb_halo_bytes.argtypes = [vp]
+        L.tslb_halo_bytes.restype = ctypes.c_longlong
+        L.tslb_halo_pack.argtypes = [vp, ip, vp]
+        L.tslb_halo_pack.restype = ip
+        L.tslb_halo_unpack.argtypes = [vp, ip, vp]
+        L.tslb_halo_unpack.restype = ip
         L.tslb_ensemble_create.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ip, ctypes.POINTER(vp)]
         L.tslb_ensemble_create.restype = ip
         L.tslb_ensemble_destroy.argtypes = [vp]

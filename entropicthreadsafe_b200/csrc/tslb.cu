@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -14,7 +15,9 @@
 
 #include "../../include/tslb.h"
 #include "../../include/tslb_io.h"
+#include "step_launch.h"
 #include "tslb_internal.h"
+#include "tslb_pair.cuh"
 #include "tslb_step.cuh"
 
 using namespace tslb;
@@ -85,6 +88,9 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
     a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = c->N;
     a.in = in; a.out = out; a.nrm = c->nrm;
     a.zchunk = c->zchunk;
+    a.zt0 = c->zt0;
+    a.zt1 = c->zt1 > 0 ? c->zt1 : c->nz;
+    a.zoff = c->z_begin - c->zt0;
     a.mode = c->p.mode;
     a.omega_pf = 1.0f / c->p.tau_a;
     a.inv_nu_a = 3.0f / (c->p.tau_a - 0.5f);
@@ -451,6 +457,8 @@ int check_flags(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+int storage_bytes(int prec) { return prec == TSLB_PREC_FP32 ? 4 : 2; }
+
 // Call fn with a value of the storage type of precision `prec`.
 template <class Fn>
 void with_storage(int prec, Fn&& fn) {
@@ -459,15 +467,19 @@ void with_storage(int prec, Fn&& fn) {
     else fn(float{});
 }
 
-int storage_bytes(int prec) { return prec == TSLB_PREC_FP32 ? 4 : 2; }
+
+}  // namespace
 
 // The step kernels use more than 48 KB of dynamic shared memory, which needs
 // a function attribute once per kernel and device.  Modules load lazily, so
 // the attribute is set only for the instantiations a lattice launches: at
 // its first launch, or earlier through prepare_step_kernel (before a stream
 // capture, for instance).
+namespace tslb_launch {
+namespace {
 std::mutex g_attr_mu;
 std::vector<std::pair<int, const void*>> g_attr_done;
+}  // namespace
 
 cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
     int dev = 0;
@@ -480,6 +492,9 @@ cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
     if (e == cudaSuccess) g_attr_done.emplace_back(dev, fn);
     return e;
 }
+}  // namespace tslb_launch
+
+namespace {
 
 // The lattices' large buffers (state, conversion and output fields, normals)
 // come from one memory pool per device that keeps freed memory for the next
@@ -537,12 +552,31 @@ int ensure_normals(tslb_ctx* c) {
     return TSLB_OK;
 }
 
+// Which step kernel a lattice uses: the paired-column kernel (tslb_pair.cuh,
+// two x columns per thread on the paired FP32 instructions) when its rows are
+// whole 16-byte chunks and it has no interior solid mask, else the scalar
+// kernel (tslb_step.cuh).  TSLB_STEP_KERNEL=scalar in the environment forces
+// the scalar kernel for every lattice created afterwards (comparison runs).
+bool force_scalar_kernel() {
+    const char* e = std::getenv("TSLB_STEP_KERNEL");
+    return e && std::strcmp(e, "scalar") == 0;
+}
+bool use_pair_kernel(int nx, int prec, bool solid, bool scalar) {
+    return !scalar && !solid && nx % (16 / storage_bytes(prec)) == 0;
+}
+// tile columns of the grid and resident blocks per SM of each kernel
+long long step_tiles(int nx, int ny, bool pair) {
+    return pair ? (long long)((nx + PX - 1) / PX) * ((ny + PY - 1) / PY)
+                : (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+}
+int step_blocks_per_sm(bool pair) { return pair ? 1 : 2; }
+
 // Target planes per block.  Each chunk also reads the source planes just
 // outside it, so long chunks repeat less work; the chunks per tile column
-// are the fewest whose blocks fill the resident slots (two blocks per SM) in
+// are the fewest whose blocks fill the resident slots (bps blocks per SM) in
 // whole waves to at least 90%, with chunks of at least 8 planes.
-int choose_zchunk(long long tiles, int nz, int sms) {
-    const long long slots = 2LL * sms;
+int choose_zchunk(long long tiles, int nz, int sms, int bps) {
+    const long long slots = (long long)bps * sms;
     const int max_chunks = std::max(1, nz / 8);
     int best = 1;
     double best_fill = -1.0;
@@ -579,38 +613,14 @@ int launch_normals(tslb_ctx* c) {
 // correction and solid mask of `a`.  launch = false only sets its shared
 // memory attribute.  Returns the error of that attribute; launch errors are
 // left to cudaGetLastError.
-cudaError_t launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st, bool launch = true) {
-    dim3 block(TX, TY, 1);
-    dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY, (a.nz + a.zchunk - 1) / a.zchunk);
-    cudaError_t err = cudaSuccess;
-    with_storage(prec, [&](auto tag) {
-        using T = decltype(tag);
-        const bool vec = a.nx % (16 / (int)sizeof(T)) == 0;
-        const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
-        auto go = [&](void (*kernel)(const StepArgs)) {
-            err = ensure_smem_attr((const void*)kernel, sm);
-            if (err == cudaSuccess && launch) kernel<<<grid, block, sm, st>>>(a);
-        };
-        if (a.solid && std::is_same<T, float>::value) {
-            // interior solid nodes (FP32 storage, no tau correction; checked by tslb_set_solid_mask)
-            if (mode == TSLB_MODE_COLOUR) go(vec ? step_kernel<TSLB_MODE_COLOUR, true, float, false, true>
-                                                 : step_kernel<TSLB_MODE_COLOUR, false, float, false, true>);
-            else if (mode == TSLB_MODE_SINGLE) go(vec ? step_kernel<TSLB_MODE_SINGLE, true, float, false, true>
-                                                      : step_kernel<TSLB_MODE_SINGLE, false, float, false, true>);
-            else go(vec ? step_kernel<TSLB_MODE_PHASEFIELD, true, float, false, true>
-                        : step_kernel<TSLB_MODE_PHASEFIELD, false, float, false, true>);
-        } else if (mode == TSLB_MODE_COLOUR && a.dtau && std::is_same<T, float>::value) {
-            // per-node tau correction (FP32 storage only; checked by the callers)
-            go(vec ? step_kernel<TSLB_MODE_COLOUR, true, float, true> : step_kernel<TSLB_MODE_COLOUR, false, float, true>);
-        } else if (mode == TSLB_MODE_COLOUR) {
-            go(vec ? step_kernel<TSLB_MODE_COLOUR, true, T> : step_kernel<TSLB_MODE_COLOUR, false, T>);
-        } else if (mode == TSLB_MODE_SINGLE) {
-            go(vec ? step_kernel<TSLB_MODE_SINGLE, true, T> : step_kernel<TSLB_MODE_SINGLE, false, T>);
-        } else {
-            go(vec ? step_kernel<TSLB_MODE_PHASEFIELD, true, T> : step_kernel<TSLB_MODE_PHASEFIELD, false, T>);
-        }
-    });
-    return err;
+cudaError_t launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st, bool launch = true,
+                               bool scalar = false) {
+    if (use_pair_kernel(a.nx, prec, a.solid != nullptr, scalar)) {
+        if (prec == TSLB_PREC_BF16) return tslb_launch::pair_step_bf16(a, mode, st, launch);
+        if (prec == TSLB_PREC_FP16S) return tslb_launch::pair_step_f16(a, mode, st, launch);
+        return tslb_launch::pair_step_f32(a, mode, st, launch);
+    }
+    return tslb_launch::scalar_step(a, mode, prec, st, launch);
 }
 
 int launch_moment_bcs(tslb_ctx* c) {
@@ -645,7 +655,7 @@ int launch_step(tslb_ctx* c) {
         if (rc) return rc;
     }
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream));
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, true, c->scalar_kernel));
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
@@ -713,7 +723,7 @@ int ensure_dtau(tslb_ctx* c) {
 
 int prepare_step_kernel(tslb_ctx* c) {
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, false));
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, false, c->scalar_kernel));
     return TSLB_OK;
 }
 
@@ -813,8 +823,13 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    c->zchunk = choose_zchunk((long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY), nz, sms);
-    if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false)) != cudaSuccess)
+    c->scalar_kernel = force_scalar_kernel();
+    {
+        const bool pair = use_pair_kernel(nx, p->precision, false, c->scalar_kernel);
+        c->zchunk = choose_zchunk(step_tiles(nx, ny, pair), nz, sms, step_blocks_per_sm(pair));
+    }
+    if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false,
+                                c->scalar_kernel)) != cudaSuccess)
         return bail(e, "cudaFuncSetAttribute");
     *out = c;
     return TSLB_OK;
@@ -831,6 +846,7 @@ void tslb_destroy(tslb_ctx* c) {
     cudaFree(c->flags);
     cudaFree(c->red);
     cudaFreeHost(c->red_host);
+    cudaFreeHost(c->red_ring);
     cudaFree(c->dtau);
     cudaFree(c->dtau_base);
     cudaFree(c->solid);
@@ -984,23 +1000,42 @@ int tslb_download_normals(tslb_ctx* c, float* nx, float* ny, float* nz) {
     return TSLB_OK;
 }
 
-int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
-    if (!c || !out) return fail(c, TSLB_ERR_ARG, "tslb_reduce: NULL");
-    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "reduce before an upload");
+}  // extern "C"
+
+namespace {
+
+// the nodes a context owns: all of them, or a z slab's own planes
+void owned_nodes(const tslb_ctx* c, long long* off, long long* n) {
+    const long long plane = (long long)c->nx * c->ny;
+    const int zt1 = c->zt1 > 0 ? c->zt1 : c->nz;
+    *off = (long long)c->zt0 * plane;
+    *n = (long long)(zt1 - c->zt0) * plane;
+}
+
+// queue the FP64 reduction of the current state and its copy into host_dst
+// (RED_PARTS doubles; page-locked for an asynchronous copy)
+int enqueue_reduce(tslb_ctx* c, double* host_dst) {
     const float* view = nullptr;
     int rc = fp32_view(c, &view);
     if (rc) return rc;
+    long long off = 0, n = 0;
+    owned_nodes(c, &off, &n);
     double* results = c->red + (size_t)c->red_blocks * RED_PARTS;
     unsigned int* ticket = reinterpret_cast<unsigned int*>(results + RED_PARTS);
-    reduce_kernel<<<(unsigned)c->red_blocks, RED_THREADS, 0, c->stream>>>(view, c->n, c->N, c->p.mode == TSLB_MODE_COLOUR,
+    reduce_kernel<<<(unsigned)c->red_blocks, RED_THREADS, 0, c->stream>>>(view + off, n, c->N, c->p.mode == TSLB_MODE_COLOUR,
                                                                           c->red, results, ticket);
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
-    CUDA_TRY(c, cudaMemcpyAsync(c->red_host, results, sizeof(double) * RED_PARTS, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    const double* h = c->red_host;
+    CUDA_TRY(c, cudaMemcpyAsync(host_dst, results, sizeof(double) * RED_PARTS, cudaMemcpyDeviceToHost, c->stream));
+    return TSLB_OK;
+}
+
+// the TSLB_RED_* values of one copied reduction
+void finish_reduce(const tslb_ctx* c, const double* h, double* out) {
+    long long off = 0, n = 0;
+    owned_nodes(c, &off, &n);
     const double umax2 = h[RED_SLOTS];
-    out[TSLB_RED_MASS] = (double)c->n + h[0];
+    out[TSLB_RED_MASS] = (double)n + h[0];
     out[TSLB_RED_MASS_A] = h[1];
     out[TSLB_RED_MASS_B] = h[2];
     out[TSLB_RED_MOM_X] = h[3];
@@ -1012,6 +1047,44 @@ int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
     out[TSLB_RED_RHO_OUT] = h[10] > 0 ? h[9] / h[10] : 0.0;
     out[TSLB_RED_DP] = (h[8] > 0 && h[10] > 0) ? (out[TSLB_RED_RHO_IN] - out[TSLB_RED_RHO_OUT]) / 3.0 : 0.0;
     out[TSLB_RED_N_IN] = h[8];
+}
+
+}  // namespace
+
+extern "C" {
+
+int tslb_reduce(tslb_ctx* c, double out[TSLB_NREDUCE]) {
+    if (!c || !out) return fail(c, TSLB_ERR_ARG, "tslb_reduce: NULL");
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "reduce before an upload");
+    int rc = enqueue_reduce(c, c->red_host);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    finish_reduce(c, c->red_host, out);
+    return check_flags(c);
+}
+
+int tslb_reduce_async(tslb_ctx* c) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!c->loaded) return fail(c, TSLB_ERR_STATE, "reduce before an upload");
+    if (c->red_queued >= TSLB_REDUCE_QUEUE)
+        return fail(c, TSLB_ERR_STATE, "tslb_reduce_async: TSLB_REDUCE_QUEUE results wait; call tslb_reduce_collect");
+    if (!c->red_ring)
+        CUDA_TRY(c, cudaMallocHost(&c->red_ring, sizeof(double) * RED_PARTS * TSLB_REDUCE_QUEUE));
+    int rc = enqueue_reduce(c, c->red_ring + (size_t)c->red_queued * RED_PARTS);
+    if (rc) return rc;
+    c->red_queued++;
+    return TSLB_OK;
+}
+
+int tslb_reduce_collect(tslb_ctx* c, double* out, int max, int* count) {
+    if (!c) return TSLB_ERR_ARG;
+    if (count) *count = 0;
+    if (max > 0 && !out) return fail(c, TSLB_ERR_ARG, "tslb_reduce_collect: NULL output");
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    const int k = std::min(std::max(max, 0), c->red_queued);
+    for (int i = 0; i < k; ++i) finish_reduce(c, c->red_ring + (size_t)i * RED_PARTS, out + (size_t)i * TSLB_NREDUCE);
+    if (count) *count = k;
+    c->red_queued = 0;
     return check_flags(c);
 }
 
@@ -1048,6 +1121,8 @@ int tslb_set_moment_bc(tslb_ctx* c, int face, int kind, float uwall, float radiu
     if (face != 4 && face != 5) return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_moment_bc: z faces (4, 5) only");
     if (kind < TSLB_MBC_NONE || kind > TSLB_MBC_JET) return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: unknown kind");
     if (c->nz < 3) return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: nz must be >= 3");
+    if ((face == 4 && c->halo_lo) || (face == 5 && c->halo_hi))
+        return fail(c, TSLB_ERR_UNSUPPORTED, "tslb_set_moment_bc: the face belongs to a neighbouring slab");
     if (!std::isfinite(uwall) || !std::isfinite(radius) || !std::isfinite(amp))
         return fail(c, TSLB_ERR_ARG, "tslb_set_moment_bc: non-finite argument");
     c->mbc_kind[face] = kind;
@@ -1300,8 +1375,10 @@ int noalloc_fail(int code, const std::string& msg) {
     return code;
 }
 
-// Once per device, with that device current: resolve the scratch address
-// and set the step kernels' shared-memory attribute.
+// Once per device, with that device current: resolve the scratch addresses
+// and set the shared-memory attribute of every step kernel the entry point
+// can launch (FP32 storage, the three modes, x aligned to 16 bytes or not),
+// so later calls make no first-use runtime calls of their own.
 int noalloc_setup(int dev, NoallocScratch** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoallocScratch& s = g_noalloc[dev];
@@ -1310,10 +1387,26 @@ int noalloc_setup(int dev, NoallocScratch** out) {
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(normals): ") + cudaGetErrorString(e));
         e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(flags): ") + cudaGetErrorString(e));
+        const int modes[3] = {TSLB_MODE_PHASEFIELD, TSLB_MODE_COLOUR, TSLB_MODE_SINGLE};
+        for (int mode : modes) {
+            for (int nx : {4, 3}) {   // 16-byte aligned rows, and not
+                StepArgs a;
+                std::memset(&a, 0, sizeof(a));
+                a.nx = nx; a.ny = 1; a.nz = 1; a.zchunk = 1;
+                e = launch_step_kernel(a, mode, TSLB_PREC_FP32, nullptr, false);
+                if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("step kernel attribute: ") + cudaGetErrorString(e));
+            }
+        }
         s.ready = true;
     }
     *out = &s;
     return TSLB_OK;
+}
+
+// [a, a + bytes) and [b, b + bytes) share a byte
+bool ranges_overlap(const void* a, const void* b, unsigned long long bytes) {
+    const unsigned long long x = (unsigned long long)(uintptr_t)a, y = (unsigned long long)(uintptr_t)b;
+    return x < y + bytes && y < x + bytes;
 }
 }  // namespace
 
@@ -1326,9 +1419,19 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     if (n > TSLB_NOALLOC_MAX_NODES)
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: " + std::to_string(n) + " nodes exceed the scratch limit of " +
                                               std::to_string(TSLB_NOALLOC_MAX_NODES) + " (TSLB_NOALLOC_MAX_NODES)");
-    if (!d_in || !d_out || d_in == d_out) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be distinct device buffers");
+    if (!d_in || !d_out) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: NULL device buffer");
     if (field_stride < n || field_stride % 4 != 0)
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: field_stride must be >= nx*ny*nz and a multiple of 4");
+    if (field_stride > (1LL << 40)) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: field_stride too large");
+    // the step reads halo neighbours of d_in after it has written d_out: the
+    // two 11-field ranges must not share a byte
+    if (ranges_overlap(d_in, d_out, (unsigned long long)NF * (unsigned long long)field_stride * sizeof(float)))
+        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out overlap (each spans 11 * field_stride floats)");
+    // the phase-field normals live in the fixed scratch with the state's field
+    // stride (component k at k * field_stride): 3 strides must fit in it
+    if (p->mode == TSLB_MODE_PHASEFIELD && field_stride > TSLB_NOALLOC_MAX_NODES)
+        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: phase-field mode needs field_stride <= " +
+                                              std::to_string(TSLB_NOALLOC_MAX_NODES) + " (TSLB_NOALLOC_MAX_NODES), the scratch's normal stride");
     if (((uintptr_t)d_in | (uintptr_t)d_out) % 16 != 0)
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be 16-byte aligned");
     for (int f = 0; f < 6; ++f)
@@ -1342,9 +1445,8 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     rc = noalloc_setup(dev, &sc);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    // the flag starts at zero on every call
-    e = cudaMemsetAsync(sc->flags, 0, sizeof(unsigned int), st);
-    if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    // The non-finite flag (zero when the library loads) collects every call's
+    // result until tslb_noalloc_check reads and clears it.
     // a context-free view of the lattice for make_args
     tslb_ctx view;
     view.p = *p;
@@ -1356,8 +1458,9 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     for (int f = 0; f < NF; ++f) view.scale[f] = 1.0f;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
-    const long long want = 8LL * sms;
+    const bool pair = use_pair_kernel(nx, TSLB_PREC_FP32, false, false);
+    const long long tiles = step_tiles(nx, ny, pair);
+    const long long want = 4LL * step_blocks_per_sm(pair) * sms;
     view.zchunk = (int)std::min<long long>(nz, std::max<long long>(8, (tiles * nz + want - 1) / want));
     if (p->mode == TSLB_MODE_PHASEFIELD) {
         StepArgs an = make_args(&view, d_in, nullptr);
@@ -1372,11 +1475,177 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     return TSLB_OK;
 }
 
+extern "C" int tslb_noalloc_check(void* stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(TSLB_ERR_ARG, "tslb_noalloc_check: device ordinal out of range");
+    NoallocScratch* sc = nullptr;
+    int rc = noalloc_setup(dev, &sc);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned int h = 0;
+    // a plain host word: the copy waits for the steps queued before it on the stream
+    if ((e = cudaMemcpyAsync(&h, sc->flags, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return noalloc_fail(TSLB_ERR_CUDA, std::string("tslb_noalloc_check: ") + cudaGetErrorString(e));
+    if (h) {
+        if ((e = cudaMemsetAsync(sc->flags, 0, sizeof(unsigned int), st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return noalloc_fail(TSLB_ERR_CUDA, std::string("tslb_noalloc_check: ") + cudaGetErrorString(e));
+        return noalloc_fail(TSLB_ERR_NAN, "tslb_step_noalloc: a step produced a non-finite moment");
+    }
+    return TSLB_OK;
+}
+
+
+// ---------------------------------------------------------------- z slabs
+// A lattice split into z slabs, one per GPU (the reference's MPI domain
+// decomposition, TSLB_2C-mpi/mpi_module.f90:2120-2258: pack, isend/irecv,
+// wait, unpack).  A slab context's device array holds its own planes and
+// `halo` copies of the neighbours' planes on each side that has a
+// neighbour; the step kernels update the own planes only (zt0 .. zt1).  A
+// step reads the moments of one plane beyond its targets and phi of `halo`
+// planes beyond (colour: the gradient at the source plane; phase field: the
+// normals there, from phi one plane further), so the exchange carries the
+// 10 non-phi moments of the edge plane and phi of `halo` edge planes.
+
+namespace {
+
+int slab_halo_planes(int mode) { return mode == TSLB_MODE_PHASEFIELD ? 3 : mode == TSLB_MODE_COLOUR ? 2 : 1; }
+int slab_phi_planes(const tslb_ctx* c) { return c->p.mode == TSLB_MODE_SINGLE ? 0 : c->halo; }
+
+// buffer: [10 moment fields of one plane][nphi phi planes], storage type
+template <class T>
+__global__ void halo_pack_kernel(const T* __restrict__ st, long long N, long long plane, int zmom, int zphi0, int nphi,
+                                 T* __restrict__ buf) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)(NMOM + nphi) * plane) return;
+    const long long k = i / plane, p = i - k * plane;
+    buf[i] = k < NMOM ? st[k * N + (long long)zmom * plane + p] : st[F_PHI * N + (long long)(zphi0 + k - NMOM) * plane + p];
+}
+template <class T>
+__global__ void halo_unpack_kernel(T* __restrict__ st, long long N, long long plane, int zmom, int zphi0, int nphi,
+                                   const T* __restrict__ buf) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)(NMOM + nphi) * plane) return;
+    const long long k = i / plane, p = i - k * plane;
+    if (k < NMOM) st[k * N + (long long)zmom * plane + p] = buf[i];
+    else st[F_PHI * N + (long long)(zphi0 + k - NMOM) * plane + p] = buf[i];
+}
+
+// side 0: the slab's bottom (z-), side 1: its top (z+).  pack: the own edge
+// planes the neighbour on that side needs; unpack: the halo planes there.
+int halo_copy(tslb_ctx* c, int side, bool pack, void* buf) {
+    if (!c) return TSLB_ERR_ARG;
+    if (side != 0 && side != 1) return fail(c, TSLB_ERR_ARG, "halo: side must be 0 (z-) or 1 (z+)");
+    if (!buf) return fail(c, TSLB_ERR_ARG, "halo: NULL buffer");
+    if (c->halo == 0) return fail(c, TSLB_ERR_STATE, "halo: not a slab context (tslb_create_slab)");
+    if (pack ? false : (side == 0 ? c->halo_lo == 0 : c->halo_hi == 0))
+        return fail(c, TSLB_ERR_STATE, "halo: the slab has no neighbour on this side");
+    const long long plane = (long long)c->nx * c->ny;
+    const int H = c->halo, nphi = slab_phi_planes(c);
+    int zmom, zphi0;
+    if (pack) {
+        zmom = side == 0 ? c->zt0 : c->zt1 - 1;
+        zphi0 = side == 0 ? c->zt0 : c->zt1 - H;
+    } else {
+        zmom = side == 0 ? c->zt0 - 1 : c->zt1;
+        zphi0 = side == 0 ? c->zt0 - H : c->zt1;
+    }
+    const long long total = (long long)(NMOM + nphi) * plane;
+    const int bs = 256;
+    with_storage(c->p.precision, [&](auto tag) {
+        using T = decltype(tag);
+        T* st = static_cast<T*>(c->state[c->cur]);
+        if (pack)
+            halo_pack_kernel<T><<<(unsigned)((total + bs - 1) / bs), bs, 0, c->stream>>>(st, c->N, plane, zmom, zphi0, nphi,
+                                                                                        static_cast<T*>(buf));
+        else
+            halo_unpack_kernel<T><<<(unsigned)((total + bs - 1) / bs), bs, 0, c->stream>>>(st, c->N, plane, zmom, zphi0, nphi,
+                                                                                          static_cast<const T*>(buf));
+    });
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return TSLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tslb_create_slab(const tslb_params* p, int nx, int ny, int nz, int z_begin, int z_end, tslb_ctx** out) {
+    if (!out) return fail(nullptr, TSLB_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    std::string why;
+    int rc = validate(p, nx, ny, nz, why);
+    if (rc) return fail(nullptr, rc, "tslb_create_slab: " + why);
+    const int H = slab_halo_planes(p->mode);
+    if (z_begin < 0 || z_end > nz || z_end - z_begin < H)
+        return fail(nullptr, TSLB_ERR_ARG, "tslb_create_slab: need 0 <= z_begin, z_end <= nz and at least " +
+                                               std::to_string(H) + " own planes");
+    const bool zper = p->bc[4] == TSLB_BC_PERIODIC;
+    const bool whole = z_begin == 0 && z_end == nz;
+    const int lo = whole ? 0 : (z_begin > 0 || zper ? H : 0);
+    const int hi = whole ? 0 : (z_end < nz || zper ? H : 0);
+    tslb_params lp = *p;
+    if (lo || hi) {
+        // a side with a halo has no boundary condition of its own: the step never
+        // reaches it (its faces stay non-periodic placeholders, in pairs)
+        if (lo) lp.bc[4] = TSLB_BC_BOUNCEBACK;
+        if (hi) lp.bc[5] = TSLB_BC_BOUNCEBACK;
+        if (lp.bc[4] == TSLB_BC_PERIODIC) lp.bc[4] = TSLB_BC_BOUNCEBACK;
+        if (lp.bc[5] == TSLB_BC_PERIODIC) lp.bc[5] = TSLB_BC_BOUNCEBACK;
+        for (int f = 4; f < 6; ++f)
+            if ((f == 4 ? lo : hi) && p->bc[f] == TSLB_BC_INLET)
+                return fail(nullptr, TSLB_ERR_ARG, "tslb_create_slab: an inlet face must belong to the slab that owns it");
+    }
+    const int nzl = lo + (z_end - z_begin) + hi;
+    tslb_ctx* c = nullptr;
+    rc = tslb_create(&lp, nx, ny, nzl, &c);
+    if (rc) return rc;
+    c->nz_global = nz;
+    c->z_begin = z_begin;
+    c->halo = whole ? 0 : H;
+    c->halo_lo = lo;
+    c->halo_hi = hi;
+    c->zt0 = lo;
+    c->zt1 = lo + (z_end - z_begin);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const bool pair = use_pair_kernel(nx, p->precision, false, c->scalar_kernel);
+    c->zchunk = choose_zchunk(step_tiles(nx, ny, pair), z_end - z_begin, sms, step_blocks_per_sm(pair));
+    *out = c;
+    return TSLB_OK;
+}
+
+int tslb_slab_geometry(const tslb_ctx* c, int out[6]) {
+    if (!c || !out) return TSLB_ERR_ARG;
+    out[0] = c->nz_global > 0 ? c->nz_global : c->nz;
+    out[1] = c->z_begin;
+    out[2] = c->z_begin + ((c->zt1 > 0 ? c->zt1 : c->nz) - c->zt0);
+    out[3] = c->halo_lo;
+    out[4] = c->halo_hi;
+    out[5] = c->halo;
+    return TSLB_OK;
+}
+
+long long tslb_halo_bytes(const tslb_ctx* c) {
+    if (!c || c->halo == 0) return 0;
+    return (long long)(NMOM + slab_phi_planes(c)) * c->nx * c->ny * c->esize;
+}
+
+int tslb_halo_pack(tslb_ctx* c, int side, void* d_buf) { return halo_copy(c, side, true, d_buf); }
+int tslb_halo_unpack(tslb_ctx* c, int side, const void* d_buf) { return halo_copy(c, side, false, const_cast<void*>(d_buf)); }
+
+}  // extern "C"
+
 // ------------------------------------------------------ batched ensemble
 struct tslb_ensemble {
     std::vector<tslb_ctx*> m;          // member lattices (own state, own params)
     int mode = 0, precision = 0;
     bool vec = true;
+    bool pair = true;                  // members stepped by the paired-column kernel
     cudaStream_t stream = nullptr;
     StepArgs* d_args[2] = {nullptr, nullptr};  // per step parity: member args
     WorkItem* d_work = nullptr;
@@ -1419,7 +1688,8 @@ int ens_build(tslb_ensemble* e) {
     for (size_t d = 0; d < e->m.size(); ++d) {
         tslb_ctx* c = e->m[d];
         c->zchunk = std::min(e->zchunk, c->nz);
-        const int gx = (c->nx + TX - 1) / TX, gy = (c->ny + TY - 1) / TY, gz = (c->nz + c->zchunk - 1) / c->zchunk;
+        const int tw = e->pair ? PX : TX, th = e->pair ? PY : TY;
+        const int gx = (c->nx + tw - 1) / tw, gy = (c->ny + th - 1) / th, gz = (c->nz + c->zchunk - 1) / c->zchunk;
         for (int bz = 0; bz < gz; ++bz)
             for (int by = 0; by < gy; ++by)
                 for (int bx = 0; bx < gx; ++bx) work.push_back(WorkItem{(int)d, bx, by, bz});
@@ -1452,18 +1722,12 @@ int ens_build(tslb_ensemble* e) {
 cudaError_t ens_kernel(tslb_ensemble* e, bool launch) {
     const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
     const StepArgs* args = e->d_args[e->parity];
-    cudaError_t err = cudaSuccess;
-    with_storage(e->precision, [&](auto tag) {
-        using T = decltype(tag);
-        const size_t sm = step_smem_bytes_es(e->mode, (int)sizeof(T));
-        auto go = [&](void (*kernel)(const StepArgs*, const WorkItem*, int)) {
-            err = ensure_smem_attr((const void*)kernel, sm);
-            if (err == cudaSuccess && launch) kernel<<<grid, dim3(TX, TY, 1), sm, e->stream>>>(args, e->d_work, e->nwork);
-        };
-        if (e->mode == TSLB_MODE_COLOUR) go(e->vec ? ensemble_kernel<TSLB_MODE_COLOUR, true, T> : ensemble_kernel<TSLB_MODE_COLOUR, false, T>);
-        else go(e->vec ? ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T> : ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T>);
-    });
-    return err;
+    if (e->pair) {
+        if (e->precision == TSLB_PREC_BF16) return tslb_launch::pair_ensemble_bf16(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
+        if (e->precision == TSLB_PREC_FP16S) return tslb_launch::pair_ensemble_f16(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
+        return tslb_launch::pair_ensemble_f32(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
+    }
+    return tslb_launch::scalar_ensemble(args, e->d_work, e->nwork, grid, e->mode, e->precision, e->vec, e->stream, launch);
 }
 
 // one ensemble step on the ensemble stream (no host synchronisation)
@@ -1532,6 +1796,7 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         const int epc = 16 / storage_bytes(e->precision);
         if (dims[3 * i] % epc) e->vec = false;
     }
+    e->pair = e->vec && !e->m[0]->scalar_kernel;
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = ens_kernel(e, false);
     int dev = 0;
@@ -1542,7 +1807,7 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         tslb_ensemble_destroy(e);
         return efail(nullptr, TSLB_ERR_CUDA, msg);
     }
-    e->grid = 2 * e->sms;  // persistent: two resident blocks per SM walk the work list
+    e->grid = step_blocks_per_sm(e->pair) * e->sms;  // persistent: the resident blocks walk the work list
     int rc = ens_build(e);
     if (rc) {
         std::string msg = e->err;
@@ -1660,7 +1925,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
     }
     const int zcands[] = {8, 16, 32, 64, 128, 1 << 20};
-    const int gcands[] = {2 * e->sms, 0};
+    const int gcands[] = {step_blocks_per_sm(e->pair) * e->sms, 0};
     float best = 1e30f;
     int bz = e->zchunk, bg = e->grid;
     cudaEvent_t t0, t1;

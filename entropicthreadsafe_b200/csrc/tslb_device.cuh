@@ -93,6 +93,9 @@ struct StepArgs {
     const float* dtau;      // colour: per-node correction of tau (stride N), or null
     const unsigned int* solid;  // interior solid nodes, one bit per node (bit i & 31 of word i >> 5), or null
     const unsigned int* near;   // fluid nodes with a solid one among their 26 neighbours, same layout
+    int zt0, zt1;           // target planes [zt0, zt1) a step updates (a z slab: its own planes;
+                            // the planes outside them are halo copies of the neighbours')
+    int zoff;               // global index of local plane 0 (a z slab's offset; seeds the rounding)
     int sr;                 // 16-bit storage: store the moments with stochastic rounding
     unsigned int sr_step;   // step counter that seeds the rounding (with the node and the field)
 };

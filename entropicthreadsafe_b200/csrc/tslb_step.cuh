@@ -191,13 +191,14 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 }
 
 // Regularized or bounce-back populations entering target (x,y,z) from
-// behind non-periodic faces; Kp points at the target's own coefficients.
-template <int MODE, class T, bool TAU = false, bool SOLID = false>
-__device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y, int z,
-                                float* acc) {
-    float Kp[NCOEF];
-#pragma unroll
-    for (int c = 0; c < NCOEF; ++c) Kp[c] = coef_at(Kc, c);
+// behind non-periodic faces; Kp holds the target's own coefficients.
+// REL (the paired kernel's target-relative accumulation): Kp[K_0] holds
+// K_0 - d, dref is the target's d, and acc collects P' - dref; a source the
+// pull visited as a zero-coefficient node (behind an x or y face, or an
+// interior solid) already added -dref, so its replacement adds P' itself.
+template <int MODE, class T, bool TAU = false, bool SOLID = false, bool REL = false>
+__device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned mask, int x, int y, int z, float* acc,
+                                  float dref = 0.f) {
     // colour mode accumulates colour increments over the target's own phi
     const float pht = Kp[K_C0];
     // own raw moments (velocity faces only)
@@ -233,19 +234,20 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
         if (!solid && !msolid) continue;
         const int c2 = dx * dx + dy * dy + dz * dz;
         const float wq = wclass(c2);
-        if (MODE == TSLB_MODE_COLOUR) {
-            // The pull skips whole solid z planes, but a source behind an x or y
-            // face, or an interior solid node, is a zero-coefficient node that
-            // added w (0 - phi_t): undo it.
-            const bool xy_solid = (dx && (mask & (1u << (dx > 0 ? 0 : 1)))) || (dy && (mask & (1u << (dy > 0 ? 2 : 3))));
-            const int sz = z - dz;
-            const bool zplane_solid = a.face[4].kind != TSLB_BC_PERIODIC && (sz < 0 || sz >= a.nz);
-            if ((xy_solid && !zplane_solid) || msolid) acc[A_COL] += wq * pht;
-        }
+        // The pull skips whole solid z planes, but a source behind an x or y
+        // face, or an interior solid node, is a zero-coefficient node it visited.
+        const bool xy_solid = (dx && (mask & (1u << (dx > 0 ? 0 : 1)))) || (dy && (mask & (1u << (dy > 0 ? 2 : 3))));
+        const bool zplane_solid = a.face[4].kind != TSLB_BC_PERIODIC && (z - dz < 0 || z - dz >= a.nz);
+        const bool visited = (xy_solid && !zplane_solid) || msolid;
+        // what the replacement adds to the f accumulators for P' = P
+        auto fval = [&](float P) { return REL && !visited ? P - dref : P; };
+        // colour mode: the visited zero node added w (0 - phi_t): undo it
+        if (MODE == TSLB_MODE_COLOUR && visited) acc[A_COL] += wq * pht;
         if (vface < 0) {
             // half-way bounce-back: f_c(x) = f^post_{-c}(x)
+            // (REL: eval_P gives P' - dref, the target being its own source)
             const float P = eval_P(Kp, 1, -dx, -dy, -dz);
-            acc_dir_rt(acc, dx, dy, dz, wq * P);
+            acc_dir_rt(acc, dx, dy, dz, wq * (REL && visited ? P + dref : P));
             if (MODE == TSLB_MODE_COLOUR) {
                 // the reflected population carries the target's own colour: only the recolouring term
                 const float bc = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
@@ -265,8 +267,22 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             const int ax = vface >> 1;
             float Ub[3] = {fb.u[0], fb.u[1], fb.u[2]};
             float phib = fb.phi < -2.f ? m[F_PHI] : fb.phi;
+            // in-plane position of the ghost node the population leaves, x - c
+            // (periodic axes wrap, a non-periodic axis clamps), in the target's layer
+            int g[3] = {x, y, z};
+            {
+                const int cc[3] = {dx, dy, dz};
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    if (b == ax) continue;
+                    const int n = dimn(a, b), v = g[b] - cc[b];
+                    g[b] = (v >= 0 && v < n) ? v : (a.face[2 * b].kind == TSLB_BC_PERIODIC ? wrapi(v, n) : (v < 0 ? 0 : n - 1));
+                }
+            }
             if (fb.kind == TSLB_BC_INLET) {
-                const long long pa = plane_area(a, vface), pi = plane_index(a, vface, x, y, z);
+                // the inlet plane at the ghost node (boundary_cds_3D_module.f90:934-986:
+                // u, v, w of node (i, j, 1) feed the populations it sends)
+                const long long pa = plane_area(a, vface), pi = plane_index(a, vface, g[0], g[1], g[2]);
                 Ub[0] = __ldg(fb.plane + pi);
                 Ub[1] = __ldg(fb.plane + pa + pi);
                 Ub[2] = __ldg(fb.plane + 2 * pa + pi);
@@ -276,10 +292,9 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             }
             float Uf[3] = {Ub[0], Ub[1], Ub[2]};  // velocity of the f equilibrium
             if (fb.kind == TSLB_BC_OUTLET) {
-                // outlet: the normal velocity of the fluid node (zero gradient)
-                if (ax == 0) Uf[0] = m[F_U];
-                else if (ax == 1) Uf[1] = m[F_V];
-                else Uf[2] = m[F_W];
+                // outlet: the normal velocity of the fluid node next to the ghost
+                // node (zero gradient, :992 w(i,j,nz) = w(i,j,nz-1))
+                Uf[ax] = ld_field<T>(a, F_U + ax, nidx(a, g[0], g[1], g[2]));
             } else if (fb.kind == TSLB_BC_PRESSURE) {
                 // pressure outlet: the fluid node's velocity at density 1
                 Uf[0] = m[F_U]; Uf[1] = m[F_V]; Uf[2] = m[F_W];
@@ -316,7 +331,7 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
                                       hxzz * (u * pzz + 2.f * w * pxz) + hyzz * (v * pzz + 2.f * w * pyz)) +
                              27.f * hxyz * (u * pyz + v * pxz + w * pxy);
             const float P = feqm1 + (1.f - omega) * an;
-            acc_dir_rt(acc, dx, dy, dz, wq * P);
+            acc_dir_rt(acc, dx, dy, dz, wq * fval(P));
             if (MODE == TSLB_MODE_COLOUR) {
                 const float dphi = phib - pht;
                 acc[A_COL] += wq * fmaf(dphi, P, dphi);
@@ -327,6 +342,16 @@ __device__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc,
             }
         }
     }
+}
+
+// the same, with the target's coefficients read from the coefficient tile at Kc
+template <int MODE, class T, bool TAU = false, bool SOLID = false>
+__device__ __forceinline__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y,
+                                                int z, float* acc) {
+    float Kp[NCOEF];
+#pragma unroll
+    for (int c = 0; c < NCOEF; ++c) Kp[c] = coef_at(Kc, c);
+    boundary_target_k<MODE, T, TAU, SOLID>(a, Kp, mask, x, y, z, acc);
 }
 
 // ---- shared-memory staging geometry ----
@@ -436,8 +461,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = bx * TX, y0 = by * TY;
-    const int z0 = bz * a.zchunk;
-    const int z1 = min(z0 + a.zchunk, a.nz);
+    const int z0 = a.zt0 + bz * a.zchunk;
+    const int z1 = min(z0 + a.zchunk, a.zt1);
     const int X = x0 + tx, Y = y0 + ty;
     const bool active = X < a.nx && Y < a.ny;
     const bool xper = a.face[0].kind == TSLB_BC_PERIODIC;
@@ -704,7 +729,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 // single-component mode does not step phi (held at 1 in both buffers)
                 constexpr int nout = MODE == TSLB_MODE_SINGLE ? F_PHI : NF;
                 // 16-bit storage: stochastic rounding seeded by the node and the step
-                const unsigned int hnode = sizeof(T) == 2 ? sr_node((unsigned int)(t * plane + cn0.off), a.sr_step) : 0u;
+                const unsigned int hnode = sizeof(T) == 2 ? sr_node((unsigned int)((t + a.zoff) * plane + cn0.off), a.sr_step) : 0u;
 #pragma unroll
                 for (int f = 0; f < nout; ++f) {
                     const T st = (sizeof(T) == 2 && a.sr) ? cvt_out_sr<T>(o[f], a, f, sr_field(hnode, f)) : cvt_out<T>(o[f], a, f);

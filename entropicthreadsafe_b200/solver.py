@@ -153,6 +153,17 @@ class Lattice:
         self._check(self.L.tslb_reduce(self.h, capi.dptr(out)))
         return dict(zip(capi.RED_NAMES, out.tolist()))
 
+    def reduce_async(self) -> None:
+        """Queue the diagnostics of the state after the queued steps (no wait)."""
+        self._check(self.L.tslb_reduce_async(self.h))
+
+    def reduce_collect(self) -> list:
+        """Wait and return the queued diagnostics, oldest first."""
+        out = np.zeros((capi.REDUCE_QUEUE, capi.NREDUCE), np.float64)
+        cnt = ctypes.c_int()
+        self._check(self.L.tslb_reduce_collect(self.h, capi.dptr(out), capi.REDUCE_QUEUE, ctypes.byref(cnt)))
+        return [dict(zip(capi.RED_NAMES, row.tolist())) for row in out[:cnt.value]]
+
     @property
     def stream(self) -> int:
         return int(self.L.tslb_stream(self.h) or 0)

@@ -38,15 +38,23 @@ def empty_fields(nx: int, ny: int, nz: int) -> dict:
 
 
 def droplet(n: int = 64, radius: float = 16.0, tau: float = 0.8, sigma: float = 0.01,
-            beta: float = 0.7, width: float = 2.0):
-    """Static droplet phi = tanh((R - r)/2) at the box centre, colour mode."""
-    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=sigma, beta=beta,
-                         grad_threshold=1e-3)
+            beta: float = 0.7, width: float = 2.0, mode: int = capi.MODE_COLOUR, sharp_c: float = 0.9):
+    """Static droplet at the box centre, fully periodic.
+
+    Colour mode: phi = tanh((R - r)/2) in [-1, 1].  Phase-field mode: the
+    reference's [0, 1] convention, phi = (1 + tanh((R - r)/2))/2, with the
+    reference's sharpening coefficient 0.3 * 3 (recursive_2c_TSLB3D.f90:28)."""
+    if mode == capi.MODE_PHASEFIELD:
+        p = capi.make_params(mode=capi.MODE_PHASEFIELD, tau_a=tau, tau_b=tau, sigma=sigma, sharp_c=sharp_c)
+    else:
+        p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=sigma, beta=beta,
+                             grad_threshold=1e-3)
     f = empty_fields(n, n, n)
     c = (n - 1) / 2.0  # (n+1)/2 in 1-based indices
     z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
     r = np.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2)
-    f["phi"][:] = np.tanh((radius - r) / width)
+    t = np.tanh((radius - r) / width)
+    f["phi"][:] = 0.5 * (1.0 + t) if mode == capi.MODE_PHASEFIELD else t
     return p, f
 
 

@@ -174,6 +174,19 @@ int  tslb_download_normals(tslb_ctx* ctx, float* nx, float* ny, float* nz);
 /* FP64 diagnostics of the current state, see TSLB_RED_* (synchronises). */
 int  tslb_reduce(tslb_ctx* ctx, double out[TSLB_NREDUCE]);
 
+/* The same diagnostics without waiting: tslb_reduce_async queues the
+ * reduction of the state after the steps queued so far, and its copy into
+ * page-locked host memory of the context; tslb_reduce_collect waits for the
+ * stream and writes the queued results in queue order to
+ * out[i * TSLB_NREDUCE ...] for i < *count = min(max, queued), dropping the
+ * rest.  At most TSLB_REDUCE_QUEUE results wait at a time.  This is the
+ * reference's pattern of reading diagnostics at the print stamps
+ * (recursive_2c_TSLB3D.f90:580-599) with a result per step kept, and no
+ * host wait per step. */
+#define TSLB_REDUCE_QUEUE 256
+int  tslb_reduce_async(tslb_ctx* ctx);
+int  tslb_reduce_collect(tslb_ctx* ctx, double* out, int max, int* count);
+
 /* Set the inlet plane of face (TSLB_BC_INLET faces only): uvw_phi holds
  * four planes (u, v, w, phi) of the face's extent, Fortran order. */
 int  tslb_set_inlet(tslb_ctx* ctx, int face, const float* uvw_phi);
@@ -272,6 +285,37 @@ long long tslb_launch_count(tslb_ctx* ctx);
  * time; different contexts may be used by different threads concurrently. */
 const char* tslb_last_error(tslb_ctx* ctx);
 
+/* ---- z slabs: one lattice over several GPUs ----
+ *
+ * Replaces the reference's MPI domain decomposition and halo exchange
+ * (TSLB_2C-mpi/mpi_module.f90:2120-2258: pack, mpi_isend/mpi_irecv, wait,
+ * unpack; periodic wrap :2083-2118).  The lattice of nx*ny*nz nodes is cut
+ * along z; a slab context owns planes [z_begin, z_end) and keeps H halo
+ * planes on every side that has a neighbouring slab (a periodic z axis, or
+ * an inner cut): H = 2 in colour mode, 3 in phase-field mode, 1 in
+ * single-component mode.  Its device array holds halo_lo + (z_end -
+ * z_begin) + halo_hi planes, bottom up; the upload/download calls take and
+ * return that whole local array (host layout, Fortran order), tslb_step
+ * updates the own planes only, and tslb_reduce covers the own planes.  The
+ * z faces of the lattice apply on the slabs that own them.
+ *
+ * After every step the halos must be refreshed before the next one:
+ *   tslb_halo_pack(ctx, side, d_buf) copies the own edge planes that the
+ *   neighbour on `side` (0: z-, 1: z+) needs into the device buffer d_buf of
+ *   tslb_halo_bytes(ctx) bytes -- the 10 non-phi moments of the edge plane,
+ *   then phi of H edge planes, in the storage type;
+ *   the caller moves the buffer to that neighbour (NCCL send/recv, a peer
+ *   copy), whose tslb_halo_unpack(ctx, other side, d_buf) writes it into its
+ *   halo planes.  Both are queued on the context stream.
+ * Inlet faces and moment-space boundary planes must lie on the slab that
+ * owns their face. */
+int  tslb_create_slab(const tslb_params* p, int nx, int ny, int nz, int z_begin, int z_end, tslb_ctx** out);
+/* out = {nz (whole lattice), z_begin, z_end, halo_lo, halo_hi, H} */
+int  tslb_slab_geometry(const tslb_ctx* ctx, int out[6]);
+long long tslb_halo_bytes(const tslb_ctx* ctx);
+int  tslb_halo_pack(tslb_ctx* ctx, int side, void* d_buf);
+int  tslb_halo_unpack(tslb_ctx* ctx, int side, const void* d_buf);
+
 /* ---- batched ensemble of independent lattices ----
  *
  * Many independent lattices of different sizes (all of one mode and one
@@ -322,18 +366,30 @@ const char* tslb_ensemble_last_error(tslb_ensemble* e);
  * d_in and d_out hold the 11 fields in the library's device layout: field
  * f at d_x + f * field_stride (floats), x fastest, field 0 = rho - 1, then
  * u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi.  Both 16-byte aligned,
- * field_stride >= nx*ny*nz and a multiple of 4, d_in != d_out.  Inlet
- * faces are not supported (their planes need storage).  The work is queued
- * on `stream` (cudaStream_t, NULL = default stream) and not waited for; no
- * non-finite check is reported.
+ * field_stride >= nx*ny*nz and a multiple of 4; the two ranges of
+ * 11 * field_stride floats must not overlap.  In phase-field mode the
+ * normals share the state's field stride inside the scratch, so there
+ * field_stride <= TSLB_NOALLOC_MAX_NODES as well.  Inlet faces are not
+ * supported (their planes need storage).  The work is queued on `stream`
+ * (cudaStream_t, NULL = default stream) and not waited for.  A step that
+ * produces a non-finite moment sets a flag in the scratch; read it with
+ * tslb_noalloc_check.
  *
- * The first call on a device resolves the scratch address and sets kernel
- * attributes; make that first call before any stream capture.  All calls
- * share the one scratch array, so calls that overlap on the GPU (other
- * streams, other threads) race: order them on one stream. */
+ * The first call on a device (of this function or tslb_noalloc_check)
+ * resolves the scratch address and sets the attributes of every kernel this
+ * function launches; make that first call before any stream capture.  All
+ * calls share the one scratch array, so calls that overlap on the GPU
+ * (other streams, other threads) race: order them on one stream. */
 int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz,
                       const float* d_in, float* d_out, long long field_stride,
                       void* stream);
+
+/* Wait for `stream` (cudaStream_t, NULL = default stream) and report whether
+ * any tslb_step_noalloc step on the current device since the previous check
+ * produced a non-finite moment: TSLB_ERR_NAN if so (the flag is then
+ * cleared), TSLB_OK if not.  Allocates nothing.  Like tslb_step_noalloc it
+ * has no counterpart in the reference. */
+int tslb_noalloc_check(void* stream);
 
 #ifdef __cplusplus
 }

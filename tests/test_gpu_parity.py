@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from entropicthreadsafe_b200 import capi, workloads
-from helpers import (GOLDEN_CASES, field_errors, golden_params, load_golden, rel_err, run_gpu,
+from helpers import (GOLDEN_CASES, field_errors, golden_inlet, golden_params, load_golden, rel_err, run_gpu,
                      run_oracle, with_halo)
 
 pytestmark = pytest.mark.gpu
@@ -35,6 +35,8 @@ def test_golden_through_capi(case):
     d, meta = load_golden(case)
     nz, ny, nx = d["rho_fp64"].shape
     with Lattice(golden_params(meta), nx, ny, nz) as lat:
+        for face, planes in (golden_inlet(d) or {}).items():
+            lat.set_inlet(face, planes)
         lat.upload_pops(with_halo(d["f_fp32"]), with_halo(d["g_fp32"]))
         lat.step(meta["nsteps"])
         out = lat.download()

@@ -6,6 +6,8 @@ memory to its own pool, a time loop that must never allocate.  For them
 the library offers one entry point that allocates nothing: its scratch
 (interface normals, the non-finite flag) is a fixed device array inside
 libtslb.so, so lattices are limited to TSLB_NOALLOC_MAX_NODES nodes.
+A step that produces a non-finite moment sets a flag in that array, which
+tslb_noalloc_check reads back (and clears) on the caller's stream.
 
 These tests run that entry point twice in a row through the C-ABI and
 compare each result with the context API (tslb_create/tslb_step) on the
@@ -122,3 +124,39 @@ def test_noalloc_rejects_oversize_and_aliased_buffers():
     # input and output must differ
     rc = L.tslb_step_noalloc(ctypes.addressof(p), 4, 4, 4, ptr, ptr, 64, None)
     assert rc == capi.ERR_ARG
+    # phase field: a field stride beyond the scratch's normal stride
+    big = torch.zeros((2, 11 * (capi.NOALLOC_MAX_NODES + 64)), dtype=torch.float32, device="cuda")
+    rc = L.tslb_step_noalloc(ctypes.addressof(p), 4, 4, 4, ctypes.c_void_p(big[0].data_ptr()),
+                             ctypes.c_void_p(big[1].data_ptr()), capi.NOALLOC_MAX_NODES + 64, None)
+    assert rc == capi.ERR_ARG
+    assert b"field_stride" in L.tslb_last_error(None)
+
+
+def test_noalloc_reports_a_non_finite_step_and_allocates_nothing():
+    """A NaN written by the host into the caller's input buffer comes back as
+    TSLB_ERR_NAN from tslb_noalloc_check (once: the check clears the flag),
+    and repeated calls leave the device's free memory unchanged."""
+    import torch
+    L = capi.lib()
+    p, f = workloads.droplet(n=24, radius=6.0)
+    n = 24 ** 3
+    stride = (n + 31) // 32 * 32
+    src = to_device_layout(f, stride)
+    dst = torch.empty_like(src)
+    args = (ctypes.addressof(p), 24, 24, 24, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr()), stride, None)
+    assert L.tslb_step_noalloc(*args) == capi.OK
+    assert L.tslb_noalloc_check(None) == capi.OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert L.tslb_step_noalloc(*args) == capi.OK
+    assert L.tslb_noalloc_check(None) == capi.OK
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    host = src.cpu()
+    host[capi.FIELDS.index("u"), 24 * 24 * 12 + 24 * 12 + 12] = float("nan")
+    src.copy_(host)
+    assert L.tslb_step_noalloc(*args) == capi.OK
+    assert L.tslb_noalloc_check(None) == capi.ERR_NAN
+    assert b"non-finite" in L.tslb_last_error(None)
+    assert L.tslb_noalloc_check(None) == capi.OK
