@@ -509,7 +509,7 @@ def run_ours(args):
     tpn, tinfo = traffic_per_node()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tpn * nodes if tpn else None, "peak_kind": peak_kind,
-            "algorithmic_bytes_per_launch": alg_bytes, "kernel": "tslb::pair_kernel<colour, float>"}
+            "algorithmic_bytes_per_launch": alg_bytes, "kernel": "tslb::step_kernel<colour>"}
     if rank != 0:
         if ws > 1:
             import torch.distributed as dist

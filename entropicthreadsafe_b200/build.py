@@ -20,8 +20,8 @@ OBJ = os.path.join(CSRC, "_build")
 OUT = os.path.join(HERE, "libtslb.so")
 DRIVER_SRC = os.path.join(HERE, "driver", "tslb_run.cpp")
 DRIVER = os.path.join(HERE, "tslb_run")
-SOURCES = ["tslb.cu", "k_scalar.cu", "k_pair_f32.cu", "k_pair_bf16.cu", "k_pair_f16.cu", "closure.cu", "tslb_io.cpp"]
-HEADERS = ["tslb_device.cuh", "tslb_step.cuh", "tslb_pair.cuh", "step_launch.h", "k_pair.cuh", "tslb_internal.h", "tcgen05.cuh", "closure_mlp.cuh"]
+SOURCES = ["tslb.cu", "k_scalar.cu", "closure.cu", "tslb_io.cpp"]
+HEADERS = ["tslb_device.cuh", "tslb_step.cuh", "step_launch.h", "tslb_internal.h", "tcgen05.cuh", "closure_mlp.cuh"]
 INCLUDES = ["tslb.h", "tslb_closure.h", "tslb_io.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -21,7 +21,7 @@ BC_PERIODIC, BC_BOUNCEBACK, BC_VELOCITY, BC_INLET, BC_OUTLET, BC_PRESSURE = rang
 MBC_NONE, MBC_COPY, MBC_JET = range(3)
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
 NREDUCE = 12
-NOALLOC_MAX_NODES = 1 << 20
+NOALLOC_SCRATCH_WORDS = 64
 REDUCE_QUEUE = 256
 RED_NAMES = ("mass", "mass_a", "mass_b", "mom_x", "mom_y", "mom_z", "kinetic",
              "umax", "rho_in", "rho_out", "dp", "n_in")

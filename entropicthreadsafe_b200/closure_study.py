@@ -2,6 +2,7 @@
 vs fine plain).
 
     python -m entropicthreadsafe_b200.closure_study [--out result.json] [--shrink K]
+    python -m entropicthreadsafe_b200.closure_study --reference-only --out reference.json
 
 1. Fine plain runs (384 x 384 x 768, three inlet-noise seeds) are the
    reference: their time-averaged fields, averaged over the seeds, give the
@@ -22,12 +23,19 @@ Times are in coarse steps; the fine grid runs twice as many steps
 (acoustic scaling).  --shrink K divides the lattice sizes and the jet
 diameter by K and the step counts by K (a quick check of the pipeline;
 the physics of a shrunk jet is not the configuration's).
+
+--reference-only runs step 1 alone and writes the fine reference (seed
+mean and spread of the statistics, and the mean profiles) that
+gain_check() compares coarse runs with: the file shipped as
+data/closure_jet_fine_reference.json.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
+import warnings
 
 import numpy as np
 
@@ -134,7 +142,10 @@ def _mean_stats(runs) -> dict | None:
     out = {k: float(np.mean([s[k] for s in ok])) for k in keys}
     out["spread"] = {k: float(np.std([s[k] for s in ok]) / abs(out[k])) if len(ok) > 1 else 0.0 for k in keys}
     for k in ("wc", "r_half", "delta"):
-        out[k] = np.nanmean(np.stack([np.asarray(s[k], float) for s in ok]), axis=0)
+        # planes where no run has a value (the half width beyond the jet) stay NaN
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", category=RuntimeWarning)
+            out[k] = np.nanmean(np.stack([np.asarray(s[k], float) for s in ok]), axis=0)
     out["z"] = ok[0]["z"]
     out["window"] = ok[0]["window"]
     return out
@@ -153,6 +164,48 @@ def _summary(runs, ref) -> dict:
             entry["vs_fine"] = jetstats.compare(ms, ref)
             entry["score"] = float(np.mean([entry["vs_fine"][k] for k in SCALARS]))
     return entry
+
+
+REFERENCE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "closure_jet_fine_reference.json")
+
+
+def save_reference(ref: dict, fine_runs, path: str) -> None:
+    """The fine reference as JSON: scalars, seed spread, profiles, window."""
+    out = {k: ref[k] for k in SCALARS}
+    out["spread"] = ref["spread"]
+    out["window"] = [float(v) for v in ref["window"]]
+    for k in ("z", "wc", "r_half", "delta"):
+        out[k] = [None if not np.isfinite(v) else float(v) for v in np.asarray(ref[k], float)]
+    out["seeds"] = [r["seed"] for r in fine_runs]
+    out["gpu_s"] = float(np.mean([r["gpu_s"] for r in fine_runs]))
+    with open(path, "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
+def load_reference(path: str = REFERENCE) -> dict:
+    with open(path) as fh:
+        d = json.load(fh)
+    for k in ("z", "wc", "r_half", "delta"):
+        d[k] = np.array([np.nan if v is None else v for v in d[k]], float)
+    return d
+
+
+def gain_check(seeds, steps: int = 20000, avg_from: int = 8000, sample_every: int = 10, interval: int = 2,
+               ref: dict | None = None) -> dict:
+    """Coarse plain and coarse + the trained closure (closure.trained_closure,
+    its calibrated gain included) on the given inlet-noise seeds, against
+    the stored fine reference: the seed means' relative errors of the four
+    statistics and the profiles, and the GPU time of each form."""
+    from .closure import trained_closure
+    ref = load_reference() if ref is None else ref
+    plain = [run_jet(1, sd, steps, avg_from, sample_every, {}) for sd in seeds]
+    clo = trained_closure()
+    try:
+        closed = [run_jet(1, sd, steps, avg_from, sample_every, {}, closure=clo, interval=interval) for sd in seeds]
+    finally:
+        clo.close()
+    return dict(seeds=list(seeds), plain=_summary(plain, ref), closure=_summary(closed, ref),
+                fine_spread=ref["spread"], fine_gpu_s=ref["gpu_s"])
 
 
 def main(argv=None) -> dict:
@@ -179,6 +232,8 @@ def main(argv=None) -> dict:
     ap.add_argument("--interval", type=int, default=2, help="closure refresh interval of the coarse runs")
     ap.add_argument("--gains", type=float, nargs="*", default=[1.0, 2.0, 4.0, 8.0],
                     help="output gains of the a posteriori calibration")
+    ap.add_argument("--reference-only", action="store_true",
+                    help="only the fine runs: write their reference statistics to --out")
     args = ap.parse_args(argv)
     K = args.shrink
     over = {}
@@ -199,7 +254,8 @@ def main(argv=None) -> dict:
     fine_runs = []
     for seed in args.fine_seeds:
         train = seed in args.train_seeds
-        r = run_jet(2, seed, 2 * T, 2 * A, 2 * S, over, dataset=closure if train else held,
+        keep = None if args.reference_only else (closure if train else held)
+        r = run_jet(2, seed, 2 * T, 2 * A, 2 * S, over, dataset=keep,
                     snaps=snaps if train else snaps[-3:],
                     keep_every=args.keep_every if train else 4 * args.keep_every, pi_scale=pi_scale,
                     z_lo=args.z_lo // K)
@@ -207,6 +263,11 @@ def main(argv=None) -> dict:
         print(f"fine run seed {seed} ({'training' if train else 'held out'}): {r['gpu_s']:.1f} s GPU, "
               f"{r['samples']} samples, diverged {r['diverged_at']}", flush=True)
     ref = _mean_stats(fine_runs)
+    if args.reference_only:
+        if args.out and ref is not None:
+            save_reference(ref, fine_runs, args.out)
+        print("fine mean:", {k: ref[k] for k in SCALARS} if ref else None, "spread", ref["spread"] if ref else None)
+        return dict(reference={k: ref[k] for k in SCALARS} if ref else None, fine_runs=[_strip(r) for r in fine_runs])
     result["fine_runs"] = [_strip(r) for r in fine_runs]
     result["fine"]["mean"] = {k: ref[k] for k in SCALARS} if ref else None
     result["fine"]["spread"] = ref["spread"] if ref else None

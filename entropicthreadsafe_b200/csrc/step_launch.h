@@ -1,8 +1,8 @@
-// step_launch.h -- host-side launchers of the step and ensemble kernels.
-// Each storage type's paired kernels and the scalar kernels live in a
-// translation unit of their own (k_pair_*.cu, k_scalar.cu), so they compile
-// in parallel.  Every launcher with launch = false only sets the kernel's
-// shared-memory attribute (before a stream capture, for instance).
+// step_launch.h -- host-side launchers of the step and ensemble kernels,
+// whose instantiations live in a translation unit of their own (k_scalar.cu)
+// that compiles in parallel with the rest.  Every launcher with launch =
+// false only sets the kernel's shared-memory attribute (before a stream
+// capture, for instance).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -13,19 +13,7 @@ namespace tslb_launch {
 // set the dynamic shared-memory limit of kernel fn once per device (tslb.cu)
 cudaError_t ensure_smem_attr(const void* fn, size_t bytes);
 
-// paired-column step kernel (tslb_pair.cuh) of one storage type
-cudaError_t pair_step_f32(const tslb::StepArgs& a, int mode, cudaStream_t st, bool launch);
-cudaError_t pair_step_bf16(const tslb::StepArgs& a, int mode, cudaStream_t st, bool launch);
-cudaError_t pair_step_f16(const tslb::StepArgs& a, int mode, cudaStream_t st, bool launch);
-// its ensemble form over a work list
-cudaError_t pair_ensemble_f32(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,
-                              cudaStream_t st, bool launch);
-cudaError_t pair_ensemble_bf16(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,
-                               cudaStream_t st, bool launch);
-cudaError_t pair_ensemble_f16(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,
-                              cudaStream_t st, bool launch);
-
-// scalar step kernel (tslb_step.cuh): every storage type, x alignment,
+// step kernel (tslb_step.cuh): every storage type, x alignment,
 // tau correction and interior solid mask
 cudaError_t scalar_step(const tslb::StepArgs& a, int mode, int prec, cudaStream_t st, bool launch);
 cudaError_t scalar_ensemble(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,

@@ -17,7 +17,6 @@
 #include "../../include/tslb_io.h"
 #include "step_launch.h"
 #include "tslb_internal.h"
-#include "tslb_pair.cuh"
 #include "tslb_step.cuh"
 
 using namespace tslb;
@@ -552,24 +551,9 @@ int ensure_normals(tslb_ctx* c) {
     return TSLB_OK;
 }
 
-// Which step kernel a lattice uses: the paired-column kernel (tslb_pair.cuh,
-// two x columns per thread on the paired FP32 instructions) when its rows are
-// whole 16-byte chunks and it has no interior solid mask, else the scalar
-// kernel (tslb_step.cuh).  TSLB_STEP_KERNEL=scalar in the environment forces
-// the scalar kernel for every lattice created afterwards (comparison runs).
-bool force_scalar_kernel() {
-    const char* e = std::getenv("TSLB_STEP_KERNEL");
-    return e && std::strcmp(e, "scalar") == 0;
-}
-bool use_pair_kernel(int nx, int prec, bool solid, bool scalar) {
-    return !scalar && !solid && nx % (16 / storage_bytes(prec)) == 0;
-}
-// tile columns of the grid and resident blocks per SM of each kernel
-long long step_tiles(int nx, int ny, bool pair) {
-    return pair ? (long long)((nx + PX - 1) / PX) * ((ny + PY - 1) / PY)
-                : (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
-}
-int step_blocks_per_sm(bool pair) { return pair ? 1 : 2; }
+// tile columns of the step grid
+long long step_tiles(int nx, int ny) { return (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY); }
+constexpr int kStepBlocksPerSM = 2;   // resident step blocks per SM (registers and shared memory)
 
 // Target planes per block.  Each chunk also reads the source planes just
 // outside it, so long chunks repeat less work; the chunks per tile column
@@ -613,13 +597,7 @@ int launch_normals(tslb_ctx* c) {
 // correction and solid mask of `a`.  launch = false only sets its shared
 // memory attribute.  Returns the error of that attribute; launch errors are
 // left to cudaGetLastError.
-cudaError_t launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st, bool launch = true,
-                               bool scalar = false) {
-    if (use_pair_kernel(a.nx, prec, a.solid != nullptr, scalar)) {
-        if (prec == TSLB_PREC_BF16) return tslb_launch::pair_step_bf16(a, mode, st, launch);
-        if (prec == TSLB_PREC_FP16S) return tslb_launch::pair_step_f16(a, mode, st, launch);
-        return tslb_launch::pair_step_f32(a, mode, st, launch);
-    }
+cudaError_t launch_step_kernel(const StepArgs& a, int mode, int prec, cudaStream_t st, bool launch = true) {
     return tslb_launch::scalar_step(a, mode, prec, st, launch);
 }
 
@@ -646,16 +624,12 @@ int launch_step(tslb_ctx* c) {
         int rc = launch_moment_bcs(c);
         if (rc) return rc;
     }
-    if (c->p.mode == TSLB_MODE_PHASEFIELD) {
-        int rc = launch_normals(c);
-        if (rc) return rc;
-    }
     if (c->closure) {
         int rc = tslb_internal::closure_before_step(c);
         if (rc) return rc;
     }
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, true, c->scalar_kernel));
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream));
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     c->cur ^= 1;
@@ -723,7 +697,7 @@ int ensure_dtau(tslb_ctx* c) {
 
 int prepare_step_kernel(tslb_ctx* c) {
     StepArgs a = make_args(c, c->state[c->cur], c->state[c->cur ^ 1]);
-    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, false, c->scalar_kernel));
+    CUDA_TRY(c, launch_step_kernel(a, c->p.mode, c->p.precision, c->stream, false));
     return TSLB_OK;
 }
 
@@ -796,11 +770,8 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     // allocate alike and reuse each other's pool memory)
     if ((e = pool_alloc(reinterpret_cast<void**>(&c->rho_out), sizeof(float) * c->N, c->device, c->stream)) != cudaSuccess)
         return bail(e, "allocation (rho)");
-    // interface normals: a field of the phase-field step; colour mode only
-    // forms them for tslb_download_normals (allocated then)
-    if (p->mode == TSLB_MODE_PHASEFIELD)
-        if ((e = pool_alloc(reinterpret_cast<void**>(&c->nrm), sizeof(float) * 3 * c->N, c->device, c->stream)) != cudaSuccess)
-            return bail(e, "allocation (normals)");
+    // the step forms the interface normals it needs itself; the normal field
+    // is allocated when tslb_download_normals asks for it
     // the pool's allocations are ordered on the lattice's stream: complete them for every stream
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
     if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
@@ -823,13 +794,8 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    c->scalar_kernel = force_scalar_kernel();
-    {
-        const bool pair = use_pair_kernel(nx, p->precision, false, c->scalar_kernel);
-        c->zchunk = choose_zchunk(step_tiles(nx, ny, pair), nz, sms, step_blocks_per_sm(pair));
-    }
-    if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false,
-                                c->scalar_kernel)) != cudaSuccess)
+    c->zchunk = choose_zchunk(step_tiles(nx, ny), nz, sms, kStepBlocksPerSM);
+    if ((e = launch_step_kernel(make_args(c, c->state[0], c->state[1]), p->mode, p->precision, c->stream, false)) != cudaSuccess)
         return bail(e, "cudaFuncSetAttribute");
     *out = c;
     return TSLB_OK;
@@ -1353,17 +1319,17 @@ int tslb_checkpoint_load(tslb_ctx* c, const char* path) {
 
 
 // ------------------------------------------------- step without allocation
-// Scratch of tslb_step_noalloc: a fixed device array of this file.  In host
-// code these names are host-side stand-ins, not device addresses; the
-// addresses come from cudaGetSymbolAddress, once per device.
-static __device__ __align__(256) float g_noalloc_normals[3 * TSLB_NOALLOC_MAX_NODES];
-static __device__ __align__(256) unsigned int g_noalloc_flags[64];
+// Scratch of tslb_step_noalloc: the step kernel's non-finite flag, in a fixed
+// device array of this file (TSLB_NOALLOC_SCRATCH_WORDS words; the step
+// needs no scratch that grows with the lattice).  In host code the name is a
+// host-side stand-in, not a device address; the address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned int g_noalloc_flags[TSLB_NOALLOC_SCRATCH_WORDS];
 
 namespace {
 constexpr int kMaxDevices = 64;
 struct NoallocScratch {
     bool ready = false;
-    float* normals = nullptr;
     unsigned int* flags = nullptr;
 };
 NoallocScratch g_noalloc[kMaxDevices];
@@ -1375,7 +1341,7 @@ int noalloc_fail(int code, const std::string& msg) {
     return code;
 }
 
-// Once per device, with that device current: resolve the scratch addresses
+// Once per device, with that device current: resolve the scratch address
 // and set the shared-memory attribute of every step kernel the entry point
 // can launch (FP32 storage, the three modes, x aligned to 16 bytes or not),
 // so later calls make no first-use runtime calls of their own.
@@ -1383,9 +1349,7 @@ int noalloc_setup(int dev, NoallocScratch** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoallocScratch& s = g_noalloc[dev];
     if (!s.ready) {
-        cudaError_t e = cudaGetSymbolAddress((void**)&s.normals, g_noalloc_normals);
-        if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(normals): ") + cudaGetErrorString(e));
-        e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
+        cudaError_t e = cudaGetSymbolAddress((void**)&s.flags, g_noalloc_flags);
         if (e != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("cudaGetSymbolAddress(flags): ") + cudaGetErrorString(e));
         const int modes[3] = {TSLB_MODE_PHASEFIELD, TSLB_MODE_COLOUR, TSLB_MODE_SINGLE};
         for (int mode : modes) {
@@ -1416,9 +1380,6 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     int rc = validate(p, nx, ny, nz, why);
     if (rc) return noalloc_fail(rc, "tslb_step_noalloc: " + why);
     const long long n = (long long)nx * ny * nz;
-    if (n > TSLB_NOALLOC_MAX_NODES)
-        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: " + std::to_string(n) + " nodes exceed the scratch limit of " +
-                                              std::to_string(TSLB_NOALLOC_MAX_NODES) + " (TSLB_NOALLOC_MAX_NODES)");
     if (!d_in || !d_out) return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: NULL device buffer");
     if (field_stride < n || field_stride % 4 != 0)
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: field_stride must be >= nx*ny*nz and a multiple of 4");
@@ -1427,11 +1388,6 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     // two 11-field ranges must not share a byte
     if (ranges_overlap(d_in, d_out, (unsigned long long)NF * (unsigned long long)field_stride * sizeof(float)))
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out overlap (each spans 11 * field_stride floats)");
-    // the phase-field normals live in the fixed scratch with the state's field
-    // stride (component k at k * field_stride): 3 strides must fit in it
-    if (p->mode == TSLB_MODE_PHASEFIELD && field_stride > TSLB_NOALLOC_MAX_NODES)
-        return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: phase-field mode needs field_stride <= " +
-                                              std::to_string(TSLB_NOALLOC_MAX_NODES) + " (TSLB_NOALLOC_MAX_NODES), the scratch's normal stride");
     if (((uintptr_t)d_in | (uintptr_t)d_out) % 16 != 0)
         return noalloc_fail(TSLB_ERR_ARG, "tslb_step_noalloc: d_in and d_out must be 16-byte aligned");
     for (int f = 0; f < 6; ++f)
@@ -1452,22 +1408,14 @@ extern "C" int tslb_step_noalloc(const tslb_params* p, int nx, int ny, int nz, c
     view.p = *p;
     view.nx = nx; view.ny = ny; view.nz = nz;
     view.n = n; view.N = field_stride;
-    view.nrm = sc->normals;
     view.flags = sc->flags;
     view.stream = st;
     for (int f = 0; f < NF; ++f) view.scale[f] = 1.0f;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const bool pair = use_pair_kernel(nx, TSLB_PREC_FP32, false, false);
-    const long long tiles = step_tiles(nx, ny, pair);
-    const long long want = 4LL * step_blocks_per_sm(pair) * sms;
+    const long long tiles = step_tiles(nx, ny);
+    const long long want = 4LL * kStepBlocksPerSM * sms;
     view.zchunk = (int)std::min<long long>(nz, std::max<long long>(8, (tiles * nz + want - 1) / want));
-    if (p->mode == TSLB_MODE_PHASEFIELD) {
-        StepArgs an = make_args(&view, d_in, nullptr);
-        const int bs = 256;
-        normals_kernel<float><<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(an, sc->normals);
-        if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_fail(TSLB_ERR_CUDA, std::string("normals launch: ") + cudaGetErrorString(e));
-    }
     StepArgs a = make_args(&view, d_in, d_out);
     if ((e = launch_step_kernel(a, p->mode, TSLB_PREC_FP32, st)) != cudaSuccess)
         return noalloc_fail(TSLB_ERR_CUDA, std::string("step kernel attribute: ") + cudaGetErrorString(e));
@@ -1613,8 +1561,7 @@ int tslb_create_slab(const tslb_params* p, int nx, int ny, int nz, int z_begin, 
     c->zt1 = lo + (z_end - z_begin);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const bool pair = use_pair_kernel(nx, p->precision, false, c->scalar_kernel);
-    c->zchunk = choose_zchunk(step_tiles(nx, ny, pair), z_end - z_begin, sms, step_blocks_per_sm(pair));
+    c->zchunk = choose_zchunk(step_tiles(nx, ny), z_end - z_begin, sms, kStepBlocksPerSM);
     *out = c;
     return TSLB_OK;
 }
@@ -1645,7 +1592,6 @@ struct tslb_ensemble {
     std::vector<tslb_ctx*> m;          // member lattices (own state, own params)
     int mode = 0, precision = 0;
     bool vec = true;
-    bool pair = true;                  // members stepped by the paired-column kernel
     cudaStream_t stream = nullptr;
     StepArgs* d_args[2] = {nullptr, nullptr};  // per step parity: member args
     WorkItem* d_work = nullptr;
@@ -1688,8 +1634,7 @@ int ens_build(tslb_ensemble* e) {
     for (size_t d = 0; d < e->m.size(); ++d) {
         tslb_ctx* c = e->m[d];
         c->zchunk = std::min(e->zchunk, c->nz);
-        const int tw = e->pair ? PX : TX, th = e->pair ? PY : TY;
-        const int gx = (c->nx + tw - 1) / tw, gy = (c->ny + th - 1) / th, gz = (c->nz + c->zchunk - 1) / c->zchunk;
+        const int gx = (c->nx + TX - 1) / TX, gy = (c->ny + TY - 1) / TY, gz = (c->nz + c->zchunk - 1) / c->zchunk;
         for (int bz = 0; bz < gz; ++bz)
             for (int by = 0; by < gy; ++by)
                 for (int bx = 0; bx < gx; ++bx) work.push_back(WorkItem{(int)d, bx, by, bz});
@@ -1722,25 +1667,11 @@ int ens_build(tslb_ensemble* e) {
 cudaError_t ens_kernel(tslb_ensemble* e, bool launch) {
     const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
     const StepArgs* args = e->d_args[e->parity];
-    if (e->pair) {
-        if (e->precision == TSLB_PREC_BF16) return tslb_launch::pair_ensemble_bf16(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
-        if (e->precision == TSLB_PREC_FP16S) return tslb_launch::pair_ensemble_f16(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
-        return tslb_launch::pair_ensemble_f32(args, e->d_work, e->nwork, grid, e->mode, e->stream, launch);
-    }
     return tslb_launch::scalar_ensemble(args, e->d_work, e->nwork, grid, e->mode, e->precision, e->vec, e->stream, launch);
 }
 
 // one ensemble step on the ensemble stream (no host synchronisation)
 int ens_launch(tslb_ensemble* e) {
-    if (e->mode == TSLB_MODE_PHASEFIELD) {
-        for (tslb_ctx* c : e->m) {
-            StepArgs a = make_args(c, c->state[c->cur ^ e->parity], nullptr);
-            const int bs = 256;
-            with_storage(e->precision, [&](auto tag) {
-                normals_kernel<decltype(tag)><<<(unsigned)((c->n + bs - 1) / bs), bs, 0, e->stream>>>(a, c->nrm);
-            });
-        }
-    }
     ECUDA_TRY(e, ens_kernel(e, true));
     ECUDA_TRY(e, cudaGetLastError());
     e->parity ^= 1;
@@ -1796,7 +1727,6 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         const int epc = 16 / storage_bytes(e->precision);
         if (dims[3 * i] % epc) e->vec = false;
     }
-    e->pair = e->vec && !e->m[0]->scalar_kernel;
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = ens_kernel(e, false);
     int dev = 0;
@@ -1807,7 +1737,7 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         tslb_ensemble_destroy(e);
         return efail(nullptr, TSLB_ERR_CUDA, msg);
     }
-    e->grid = step_blocks_per_sm(e->pair) * e->sms;  // persistent: the resident blocks walk the work list
+    e->grid = kStepBlocksPerSM * e->sms;  // persistent: the resident blocks walk the work list
     int rc = ens_build(e);
     if (rc) {
         std::string msg = e->err;
@@ -1925,7 +1855,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
     }
     const int zcands[] = {8, 16, 32, 64, 128, 1 << 20};
-    const int gcands[] = {step_blocks_per_sm(e->pair) * e->sms, 0};
+    const int gcands[] = {kStepBlocksPerSM * e->sms, 0};
     float best = 1e30f;
     int bz = e->zchunk, bg = e->grid;
     cudaEvent_t t0, t1;

@@ -193,13 +193,33 @@ __device__ __forceinline__ T cvt_out(float v, const StepArgs& a, int f) {
     else return Stor<T>::st(v);
 }
 
+// largest finite value of a 16-bit storage type (bf16: FP32's range)
+template <class T>
+struct Stor16Max;
+template <>
+struct Stor16Max<__half> {
+    static constexpr float value = 65504.0f;
+};
+template <>
+struct Stor16Max<__nv_bfloat16> {
+    static constexpr float value = 3.3895313892515355e38f;
+};
+template <class T>
+__device__ __forceinline__ T bits_as(unsigned short u);
+template <>
+__device__ __forceinline__ __half bits_as<__half>(unsigned short u) { return __ushort_as_half(u); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 bits_as<__nv_bfloat16>(unsigned short u) { return __ushort_as_bfloat16(u); }
+
 // Stochastic rounding of the 16-bit stored moments: a value rounds away from
 // zero with the probability of its distance from the value toward zero, so
 // the expected stored value is the FP32 one.  Rounding to nearest drops every
 // change smaller than half a unit in the last place at every step - the body
 // force of the channel adds about 2.5e-6 to u per step, 1/200 of a BF16 unit
-// at u = 0.07 - and the stored flow stops following the forcing.  The random
-// bits hash the node, the field and the step counter, so a run (and its
+// at u = 0.07 - and the stored flow stops following the forcing.  The step
+// stores two fields with one stochastically rounded hardware conversion
+// (cvt.rs.bf16x2.f32 / cvt.rs.f16x2.f32, sm_100a) whose random bits hash the
+// node, the pair's first field and the step counter, so a run (and its
 // restart from a checkpoint) is reproducible.
 __device__ __forceinline__ unsigned int sr_node(unsigned int node, unsigned int step) {
     unsigned int h = node * 0x9E3779B1u ^ (step * 0x85EBCA77u + 0x165667B1u);
@@ -212,27 +232,29 @@ __device__ __forceinline__ unsigned int sr_field(unsigned int hnode, int f) {
     unsigned int h = (hnode + (unsigned int)f * 0x9E3779B9u) * 0x85EBCA6Bu;
     return h ^ (h >> 16);
 }
-// BF16: add 16 random bits below the kept mantissa, then truncate (the sign
-// stays, so magnitudes round up); non-finite values pass unchanged
-__device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned int r) {
-    unsigned int b = __float_as_uint(v);
-    if ((b & 0x7F800000u) != 0x7F800000u) b += r & 0xFFFFu;
-    return __ushort_as_bfloat16((unsigned short)(b >> 16));
-}
-// FP16 (of the scaled value x): the hardware's stochastically rounded
-// conversion (cvt.rs, sm_100a) with the random bits r; the value fills both
-// halves and the low half is kept
-__device__ __forceinline__ __half f16_sr(float x, unsigned int r) {
-    unsigned int d;
-    asm("cvt.rs.f16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(x), "r"(r));
-    return __ushort_as_half((unsigned short)(d & 0xFFFFu));
-}
+// Store fields f and g (g == f: f alone) of one node in 16-bit storage with
+// one paired conversion: cvt.rn / cvt.rs (stochastic, random bits r) to
+// f16x2 or bf16x2 of the stored values (fp16: value * per-field scale).
+// Returns the largest stored magnitude before rounding, for the range check.
 template <class T>
-__device__ __forceinline__ T cvt_out_sr(float v, const StepArgs& a, int f, unsigned int r) {
-    if constexpr (std::is_same<T, __half>::value) return f16_sr(v * a.scale[f], r);
-    else if constexpr (std::is_same<T, __nv_bfloat16>::value) return bf16_sr(v, r);
-    else return v;
+__device__ __forceinline__ float store_pair16(T* po, const StepArgs& a, int f, int g, float vf, float vg, int sr,
+                                              unsigned int r) {
+    constexpr bool H = std::is_same<T, __half>::value;
+    const float xf = H ? vf * a.scale[f] : vf, xg = H ? vg * a.scale[g] : vg;
+    unsigned int d;
+    if (sr) {
+        if (H) asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(xg), "f"(xf), "r"(r));
+        else asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(xg), "f"(xf), "r"(r));
+    } else {
+        if (H) asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(xg), "f"(xf));
+        else asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(xg), "f"(xf));
+    }
+    // the low half holds field f, the high half field g
+    po[f * a.N] = bits_as<T>((unsigned short)(d & 0xFFFFu));
+    if (g != f) po[g * a.N] = bits_as<T>((unsigned short)(d >> 16));
+    return fmaxf(fabsf(xf), fabsf(xg));
 }
+
 template <class T>
 __device__ __forceinline__ float ld_field(const StepArgs& a, int f, long long idx) {
     return cvt_in<T>(__ldg(reinterpret_cast<const T*>(a.in) + f * a.N + idx), a, f);
@@ -259,20 +281,6 @@ __device__ float phi_at(const StepArgs& a, int x, int y, int z) {
     if (fb.kind == TSLB_BC_INLET) return __ldg(fb.plane + 3 * plane_area(a, face) + plane_index(a, face, c[0], c[1], c[2]));
     if (a.wall_phi_mode == 0) return fb.phi;
     return ld_field<T>(a, F_PHI, nidx(a, c[0], c[1], c[2]));
-}
-
-// normal component `comp` at any node: periodic wrap, zero on solid faces
-__device__ inline float nrm_at(const StepArgs& a, int comp, int x, int y, int z) {
-    int c[3] = {x, y, z};
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-        int n = dimn(a, ax);
-        if (c[ax] < 0 || c[ax] >= n) {
-            if (a.face[2 * ax].kind != TSLB_BC_PERIODIC) return 0.0f;
-            c[ax] = wrapi(c[ax], n);
-        }
-    }
-    return __ldg(a.nrm + comp * a.N + nidx(a, c[0], c[1], c[2]));
 }
 
 __device__ __forceinline__ bool interior1(const StepArgs& a, int x, int y, int z) {
@@ -304,32 +312,14 @@ __device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
     g[2] = 3.f * gz;
 }
 
-// -div(n) with the same stencil (recursive_2c_TSLB3D.f90:617-627)
-__device__ inline float curvature_at(const StepArgs& a, int x, int y, int z) {
-    float div = 0.f;
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-        for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
-                if (dx == 0 && dy == 0 && dz == 0) continue;
-                const float wv = wclass(dx * dx + dy * dy + dz * dz);
-                float t = 0.f;
-                if (dx) t += dx * nrm_at(a, 0, x + dx, y + dy, z + dz);
-                if (dy) t += dy * nrm_at(a, 1, x + dx, y + dy, z + dz);
-                if (dz) t += dz * nrm_at(a, 2, x + dx, y + dy, z + dz);
-                div += wv * t;
-            }
-    return -3.f * div;
-}
-
 // Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms.
-// m[] are the node's 11 moments (m[F_D] = rho - 1).
+// m[] are the node's 11 moments (m[F_D] = rho - 1).  gphi: colour mode, the
+// gradient of phi; phase field, the interface normal n, with curv the
+// curvature -div n where the interface indicator exceeds 0.2 (else 0).
 // TAU: the node's relaxation time is tau(phi) + dtau[id] (a local eddy-viscosity
 // correction); the surface-tension coefficient follows the corrected omega.
 template <int MODE, bool TAU = false>
-__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, int x, int y, int z, float* K,
+__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, float curv, float* K,
                                            long long id = 0) {
     const float d = m[F_D], rho = 1.f + d;
     const float u = m[F_U], v = m[F_V], w = m[F_W];
@@ -365,12 +355,10 @@ __device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, co
         V = v + a.force[1];
         W = w + a.force[2];
     } else {
+        // CSF velocity shift u + sigma kappa n (+ F) (recursive_2c_TSLB3D.f90:630-636,
+        // lb_kernels_module.f90:769)
         omega = a.omega_pf;
-        const long long id = nidx(a, x, y, z);
-        const float n0 = __ldg(a.nrm + id), n1 = __ldg(a.nrm + a.N + id), n2 = __ldg(a.nrm + 2 * a.N + id);
-        float curv = 0.f;
-        const float ind = phi * (1.f - phi) * (n0 * n0 + n1 * n1 + n2 * n2);
-        if (ind > 0.2f) curv = curvature_at(a, x, y, z);
+        const float n0 = gphi[0], n1 = gphi[1], n2 = gphi[2];
         const float sk = a.sigma * curv;
         U = u + sk * n0 + a.force[0];
         V = v + sk * n1 + a.force[1];

@@ -40,7 +40,6 @@ struct tslb_ctx {
     // halo_lo + owned + halo_hi planes; a step updates planes [zt0, zt1)
     int zt0 = 0, zt1 = 0;                  // zt1 = 0: all planes
     int nz_global = 0, z_begin = 0, halo = 0, halo_lo = 0, halo_hi = 0;
-    bool scalar_kernel = false;            // TSLB_STEP_KERNEL=scalar at creation
     long long launches = 0;
     // per-node tau correction (colour mode, FP32 storage): dtau_base is the
     // static field of tslb_set_tau_correction (e.g. a sponge layer); with a

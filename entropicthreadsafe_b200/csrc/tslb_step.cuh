@@ -102,17 +102,27 @@ __host__ __device__ constexpr float w1d(int c) { return c == 0 ? 2.0f / 3.0f : 1
 
 // Moments of the three populations of one (cy, cz) group: directions
 // (+1, cy, cz), (0, cy, cz), (-1, cy, cz) with values a, c0, b (unweighted
-// P'), folded through S = a + b and D = a - b before accumulation.
+// P'), folded through S = a + b, D = a - b and T = S + (wC/wE) c0, each
+// accumulated with the weight wE of the x-moving directions (wC/wE = 4).
 template <int CYv, int CZv>
 __device__ __forceinline__ void acc_group(float* acc, float a, float c0, float b) {
-    constexpr float wE = w1d(1) * w1d(CYv) * w1d(CZv), wC = w1d(0) * w1d(CYv) * w1d(CZv);
-    const float S = wE * (a + b), D = wE * (a - b), T = fmaf(wC, c0, S);
-    acc[A_RHO] += T;
-    acc[A_JX] += D;
-    acc[A_XX] += S;
-    if (CYv) { acc[A_JY] += CYv > 0 ? T : -T; acc[A_YY] += T; acc[A_XY] += CYv > 0 ? D : -D; }
-    if (CZv) { acc[A_JZ] += CZv > 0 ? T : -T; acc[A_ZZ] += T; acc[A_XZ] += CZv > 0 ? D : -D; }
-    if (CYv && CZv) acc[A_YZ] += (CYv * CZv) > 0 ? T : -T;
+    constexpr float wE = w1d(1) * w1d(CYv) * w1d(CZv);
+    constexpr float pe = wE, ne = -wE;
+    const float S = a + b, D = a - b, T = fmaf(w1d(0) / w1d(1), c0, S);
+    acc[A_RHO] = fmaf(pe, T, acc[A_RHO]);
+    acc[A_JX] = fmaf(pe, D, acc[A_JX]);
+    acc[A_XX] = fmaf(pe, S, acc[A_XX]);
+    if (CYv) {
+        acc[A_JY] = fmaf(CYv > 0 ? pe : ne, T, acc[A_JY]);
+        acc[A_YY] = fmaf(pe, T, acc[A_YY]);
+        acc[A_XY] = fmaf(CYv > 0 ? pe : ne, D, acc[A_XY]);
+    }
+    if (CZv) {
+        acc[A_JZ] = fmaf(CZv > 0 ? pe : ne, T, acc[A_JZ]);
+        acc[A_ZZ] = fmaf(pe, T, acc[A_ZZ]);
+        acc[A_XZ] = fmaf(CZv > 0 ? pe : ne, D, acc[A_XZ]);
+    }
+    if (CYv && CZv) acc[A_YZ] = fmaf(CYv * CZv > 0 ? pe : ne, T, acc[A_YZ]);
 }
 
 // colour of one (cy, cz) group, as an increment over the target's own
@@ -192,13 +202,8 @@ __device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* ac
 
 // Regularized or bounce-back populations entering target (x,y,z) from
 // behind non-periodic faces; Kp holds the target's own coefficients.
-// REL (the paired kernel's target-relative accumulation): Kp[K_0] holds
-// K_0 - d, dref is the target's d, and acc collects P' - dref; a source the
-// pull visited as a zero-coefficient node (behind an x or y face, or an
-// interior solid) already added -dref, so its replacement adds P' itself.
-template <int MODE, class T, bool TAU = false, bool SOLID = false, bool REL = false>
-__device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned mask, int x, int y, int z, float* acc,
-                                  float dref = 0.f) {
+template <int MODE, class T, bool TAU = false, bool SOLID = false>
+__device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned mask, int x, int y, int z, float* acc) {
     // colour mode accumulates colour increments over the target's own phi
     const float pht = Kp[K_C0];
     // own raw moments (velocity faces only)
@@ -239,15 +244,12 @@ __device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned m
         const bool xy_solid = (dx && (mask & (1u << (dx > 0 ? 0 : 1)))) || (dy && (mask & (1u << (dy > 0 ? 2 : 3))));
         const bool zplane_solid = a.face[4].kind != TSLB_BC_PERIODIC && (z - dz < 0 || z - dz >= a.nz);
         const bool visited = (xy_solid && !zplane_solid) || msolid;
-        // what the replacement adds to the f accumulators for P' = P
-        auto fval = [&](float P) { return REL && !visited ? P - dref : P; };
         // colour mode: the visited zero node added w (0 - phi_t): undo it
         if (MODE == TSLB_MODE_COLOUR && visited) acc[A_COL] += wq * pht;
         if (vface < 0) {
             // half-way bounce-back: f_c(x) = f^post_{-c}(x)
-            // (REL: eval_P gives P' - dref, the target being its own source)
             const float P = eval_P(Kp, 1, -dx, -dy, -dz);
-            acc_dir_rt(acc, dx, dy, dz, wq * (REL && visited ? P + dref : P));
+            acc_dir_rt(acc, dx, dy, dz, wq * P);
             if (MODE == TSLB_MODE_COLOUR) {
                 // the reflected population carries the target's own colour: only the recolouring term
                 const float bc = -(dx * Kp[K_C1] + dy * Kp[K_C2] + dz * Kp[K_C3]);
@@ -331,7 +333,7 @@ __device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned m
                                       hxzz * (u * pzz + 2.f * w * pxz) + hyzz * (v * pzz + 2.f * w * pyz)) +
                              27.f * hxyz * (u * pyz + v * pxz + w * pxy);
             const float P = feqm1 + (1.f - omega) * an;
-            acc_dir_rt(acc, dx, dy, dz, wq * fval(P));
+            acc_dir_rt(acc, dx, dy, dz, wq * P);
             if (MODE == TSLB_MODE_COLOUR) {
                 const float dphi = phib - pht;
                 acc[A_COL] += wq * fmaf(dphi, P, dphi);
@@ -360,14 +362,19 @@ __device__ __forceinline__ void boundary_target(const StepArgs& a, const float* 
 constexpr int NTHR = TX * TY;
 constexpr int NHALO = CAREA - NTHR;           // coefficient nodes on the tile rim (84)
 constexpr int NMOM = NF - 1;                  // moments staged per node (phi comes from the phi ring)
-template <int ES>   // element size in bytes
+// Phi rows staged beyond the tile in y (and planes held beyond the source
+// plane in z): colour mode reads the gradient at the coefficient nodes (the
+// tile plus a one-node rim), 2; the phase field also the normals of their
+// neighbours for the curvature, 3.
+__host__ __device__ constexpr int phi_halo(int mode) { return mode == TSLB_MODE_PHASEFIELD ? 3 : 2; }
+template <int ES, int PHR = 2>   // element size in bytes, phi halo
 struct Geo {
     static constexpr int EPC = 16 / ES;               // elements per 16-byte chunk
     static constexpr int SW = TX + 2 * EPC;           // staged row width
     static constexpr int OFF = EPC - 1;               // staged column of tile column 0 (x0 - 1)
     static constexpr int NCH = SW / EPC;              // chunks per row
     static constexpr int MROWS = CH;                  // moment rows: y0-1 .. y0+TY
-    static constexpr int PROWS = TY + 4;              // phi rows: y0-2 .. y0+TY+1
+    static constexpr int PROWS = TY + 2 * PHR;        // phi rows: y0-PHR .. y0+TY+PHR-1
     static constexpr int MAREA = MROWS * SW, PAREA = PROWS * SW;
     static constexpr int MCELLS = MROWS * NCH;        // 16-byte cells of one staged moment plane
     static constexpr int MGROUPS = NTHR / MCELLS;     // thread (g, cell) copies fields g, g + MGROUPS, ...
@@ -379,12 +386,12 @@ struct Geo {
 };
 
 // Phi ring: slot z & (PRING - 1) holds phi plane z.  Iteration s stages plane
-// s+2 while other threads may still read plane s-2 (the previous iteration's
-// target plane s-2 in its pull), so the ring holds at least 5 planes.
+// s+PHR while other threads may still read planes from s-PHR on (the previous
+// iteration's pull or curvature), so the ring holds at least 2 PHR + 1 planes.
 constexpr int PRING = 8;
 __host__ __device__ constexpr size_t step_smem_bytes_es(int mode, int es) {
     return sizeof(float) * 2 * NCOEF * CAREA + (size_t)es * 2 * NMOM * CH * (TX + 2 * (16 / es)) +
-           (mode == TSLB_MODE_COLOUR ? (size_t)es * PRING * (TY + 4) * (TX + 2 * (16 / es)) : 0);
+           (mode != TSLB_MODE_SINGLE ? (size_t)es * PRING * (TY + 2 * phi_halo(mode)) * (TX + 2 * (16 / es)) : 0);
 }
 __host__ __device__ constexpr size_t step_smem_bytes(int mode) { return step_smem_bytes_es(mode, 4); }
 
@@ -415,8 +422,23 @@ __device__ __forceinline__ void grad_smem(const T* pm, const T* p0, const T* pp,
     g[2] = c1 * z1 + c2 * z2 + c3 * z3;
 }
 
-// Node descriptor: in-plane offset after the periodic wrap of x and y, and
-// whether the node lies behind a non-periodic x or y face.
+// Phase-field interface normal n = g / (|g| + 1e-9) from the staged phi
+// planes (ring slots of plane z and its neighbours), at staged offset pi
+// (recursive_2c_TSLB3D.f90:555-571).
+template <int SWv, class T>
+__device__ __forceinline__ void pf_normal(const T* ring, int parea, int z, int pi, const StepArgs& a, float n[3]) {
+    const T* p0 = ring + (z & (PRING - 1)) * parea + pi;
+    const T* pm = ring + ((z - 1) & (PRING - 1)) * parea + pi;
+    const T* pp = ring + ((z + 1) & (PRING - 1)) * parea + pi;
+    grad_smem<SWv>(pm, p0, pp, n);
+    if constexpr (std::is_same<T, __half>::value) {
+        n[0] *= a.iscale[F_PHI]; n[1] *= a.iscale[F_PHI]; n[2] *= a.iscale[F_PHI];
+    }
+    const float den = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) + 1e-9f;
+    n[0] /= den; n[1] /= den; n[2] /= den;
+}
+
+
 struct XYNode {
     int off;      // gx + nx * gy (wrapped/clamped)
     int gx, gy;   // raw coordinates (may be out of range)
@@ -431,6 +453,42 @@ __device__ __forceinline__ XYNode xy_node(const StepArgs& a, int gx, int gy, boo
     if (cy < 0 || cy >= a.ny) { if (yper) cy = wrapi(cy, a.ny); else { n.out = true; cy = cy < 0 ? 0 : a.ny - 1; } }
     n.off = cx + a.nx * cy;
     return n;
+}
+
+// Phase-field curvature -div n at a coefficient node: the isotropic stencil
+// over its 26 neighbours (recursive_2c_TSLB3D.f90:617-627), each neighbour's
+// normal recomputed from the staged phi (pf_normal); a neighbour behind a
+// non-periodic face, or an interior solid one, has n = 0.  z is the source
+// plane (ring index), gz its lattice plane, pi the node's staged offset.
+template <int SWv, bool SOLID, class T>
+__device__ float pf_curvature(const T* ring, int parea, int z, int pi, const StepArgs& a, const XYNode& nd, int gz,
+                              bool xper, bool yper, bool zper) {
+    float div = 0.f;
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int zn = gz + dz;
+        if (!zper && (zn < 0 || zn >= a.nz)) continue;
+#pragma unroll 1
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yn = nd.gy + dy;
+            if (!yper && (yn < 0 || yn >= a.ny)) continue;
+#pragma unroll 1
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!dx && !dy && !dz) continue;
+                const int xn = nd.gx + dx;
+                if (!xper && (xn < 0 || xn >= a.nx)) continue;
+                if (SOLID && bit_at(a.solid, nidx(a, wrapi(xn, a.nx), wrapi(yn, a.ny), wrapi(zn, a.nz)))) continue;
+                float n[3];
+                pf_normal<SWv>(ring, parea, z + dz, pi + dy * SWv + dx, a, n);
+                float t = 0.f;
+                if (dx) t += dx * n[0];
+                if (dy) t += dy * n[1];
+                if (dz) t += dz * n[2];
+                div += wclass(dx * dx + dy * dy + dz * dz) * t;
+            }
+        }
+    }
+    return -3.f * div;
 }
 
 __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
@@ -451,12 +509,14 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // SOLID: the lattice has interior solid nodes (bit masks a.solid, a.near).
 template <int MODE, bool VEC, class T, bool TAU = false, bool SOLID = false>
 __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, int bz) {
-    using G = Geo<sizeof(T)>;
+    constexpr int PHR = phi_halo(MODE);
+    constexpr bool PHI = MODE != TSLB_MODE_SINGLE;   // phi is staged (colour, phase field)
+    using G = Geo<sizeof(T), PHR>;
     constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
     extern __shared__ float4 smem4[];
     float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NCOEF][CAREA]
     T* mst = reinterpret_cast<T*>(coef_base + 2 * NCOEF * CAREA);     // [2][NMOM][MROWS][SW]
-    T* phis = mst + 2 * NMOM * MAREA;                                 // colour: [PRING][PROWS][SW]
+    T* phis = mst + 2 * NMOM * MAREA;                                 // [PRING][PROWS][SW] (not single)
     const T* gin = reinterpret_cast<const T*>(a.in);
     T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -494,9 +554,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         ci1 = cy * CW + cx;
     }
     // position of a coefficient node (cx, cy) in the staged planes: moments
-    // row cy, column cx + OFF; phi row cy + 1, same column
+    // row cy, column cx + OFF; phi row cy + PHR - 1, same column
     const int mi0 = (ci0 / CW) * SW + (ci0 % CW) + G::OFF, mi1 = (ci1 / CW) * SW + (ci1 % CW) + G::OFF;
-    const int pi0 = mi0 + SW, pi1 = mi1 + SW;
+    const int pi0 = mi0 + (PHR - 1) * SW, pi1 = mi1 + (PHR - 1) * SW;
     const int nnodes = has_rim ? 2 : 1;
 
     auto zwrap = [&](int z, bool& out) {
@@ -505,7 +565,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         return z;
     };
 
-    // ---- staging of phi planes (colour mode) ----
+    // ---- staging of phi planes (colour and phase-field modes) ----
     // VEC: copy j < PCOPIES is the 16-byte chunk (row j / NCH, chunk j % NCH);
     // a chunk is either fully inside the domain (after the periodic wrap) or
     // fully behind a non-periodic face, whose ghost values are computed.
@@ -513,7 +573,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     bool pch_out = true;
     if (VEC && tid < G::PCOPIES) {
         const int row = tid / G::NCH, ch = tid % G::NCH;
-        const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - 2 + row, xper, yper);
+        const XYNode nd = xy_node(a, x0 - EPC + EPC * ch, y0 - PHR + row, xper, yper);
         pch_off = nd.off;
         pch_out = nd.out;
         pch_dst = row * SW + EPC * ch;
@@ -534,7 +594,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 } else {
                     const int row = tid / G::NCH, ch = tid % G::NCH;
 #pragma unroll
-                    for (int e = 0; e < EPC; ++e) dst[e] = ghost(phi_at<T>(a, x0 - EPC + EPC * ch + e, y0 - 2 + row, z));
+                    for (int e = 0; e < EPC; ++e) dst[e] = ghost(phi_at<T>(a, x0 - EPC + EPC * ch + e, y0 - PHR + row, z));
                 }
             }
         } else {
@@ -543,7 +603,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 const int j = tid + r * NTHR;
                 if (j < G::PELEMS) {
                     const int row = j / SW, col = j % SW;
-                    const XYNode nd = xy_node(a, x0 - EPC + col, y0 - 2 + row, xper, yper);
+                    const XYNode nd = xy_node(a, x0 - EPC + col, y0 - PHR + row, xper, yper);
                     if (!nd.out && !zout) {
                         if constexpr (sizeof(T) == 4) cp_async4(reinterpret_cast<float*>(slot + j), reinterpret_cast<const float*>(ph + nd.off));
                         else slot[j] = ph[nd.off];
@@ -605,11 +665,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         }
     };
 
-    if (MODE == TSLB_MODE_COLOUR) {
-        stage_phi(z0 - 2);
-        stage_phi(z0 - 1);
-        stage_phi(z0);
-    }
+    // phi of the planes the first source plane z0 - 1 reads: z0 - PHR .. z0 + PHR - 2
+    if (PHI)
+        for (int z = z0 - PHR; z <= z0 + PHR - 2; ++z) stage_phi(z);
     stage_mom(z0 - 1);
     cp_async_commit();
     cp_async_wait<0>();
@@ -623,8 +681,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     for (int s = z0 - 1; s <= z1; ++s) {
         float* coef = coef_base + buf * (NCOEF * CAREA);
         const bool more = s < z1;
-        // ---- 0. prefetch: phi of plane s+2, moments of plane s+1 ----
-        if (MODE == TSLB_MODE_COLOUR && more) stage_phi(s + 2);
+        // ---- 0. prefetch: phi of plane s+PHR, moments of plane s+1 ----
+        if (PHI && more) stage_phi(s + PHR);
         cp_async_commit();
         if (more) stage_mom(s + 1);
         cp_async_commit();
@@ -647,7 +705,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
 #pragma unroll
                 for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
                 float g[3] = {0.f, 0.f, 0.f};
-                int gx = 0, gy = 0;
+                float curv = 0.f;
                 if (MODE == TSLB_MODE_COLOUR) {
                     const T* p0 = phis + (s & (PRING - 1)) * PAREA + pi;
                     const T* pm = phis + ((s - 1) & (PRING - 1)) * PAREA + pi;
@@ -658,13 +716,18 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                         g[0] *= a.iscale[F_PHI]; g[1] *= a.iscale[F_PHI]; g[2] *= a.iscale[F_PHI];
                     }
                 } else if (MODE == TSLB_MODE_PHASEFIELD) {
-                    m[F_PHI] = ld_field<T>(a, F_PHI, (long long)gz * plane + nd.off);
-                    gx = nd.off % a.nx;
-                    gy = nd.off / a.nx;
+                    // the interface normal n = grad phi / (|grad phi| + 1e-9) of the node
+                    // (recursive_2c_TSLB3D.f90:555-571), and where the indicator
+                    // phi (1 - phi) |n|^2 exceeds 0.2, the curvature -div n over the 26
+                    // neighbours' normals, each from the staged phi (:614-629)
+                    m[F_PHI] = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
+                    pf_normal<SW>(phis, PAREA, s, pi, a, g);
+                    const float ind = m[F_PHI] * (1.f - m[F_PHI]) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+                    if (ind > 0.2f) curv = pf_curvature<SW, SOLID>(phis, PAREA, s, pi, a, nd, gz, xper, yper, zper);
                 } else {
                     m[F_PHI] = 1.f;
                 }
-                node_coefs<MODE, TAU>(a, m, g, gx, gy, gz, K, TAU ? (long long)gz * plane + nd.off : 0);
+                node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs<MODE>(coef + 2 * ci, K);
         };
@@ -683,7 +746,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
                 // own-column phi of the target planes s-1 .. s+1
-                const int po = (ty + 2) * SW + (tx + EPC);
+                const int po = (ty + PHR) * SW + (tx + EPC);
                 phm = cvt_in<T>(phis[((s - 1) & (PRING - 1)) * PAREA + po], a, F_PHI);
                 ph0 = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + po], a, F_PHI);
                 php = cvt_in<T>(phis[((s + 1) & (PRING - 1)) * PAREA + po], a, F_PHI);
@@ -725,18 +788,31 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
 #pragma unroll
                     for (int f = 0; f < NF; ++f) po[f * a.N] = pi[f * a.N];
                 } else {
-                float chk = 0.f;
                 // single-component mode does not step phi (held at 1 in both buffers)
                 constexpr int nout = MODE == TSLB_MODE_SINGLE ? F_PHI : NF;
-                // 16-bit storage: stochastic rounding seeded by the node and the step
-                const unsigned int hnode = sizeof(T) == 2 ? sr_node((unsigned int)((t + a.zoff) * plane + cn0.off), a.sr_step) : 0u;
+                bool bad;
+                if constexpr (sizeof(T) == 2) {
+                    // 16-bit storage: two fields per conversion (store_pair16), stochastic
+                    // rounding seeded by the node (its index in the whole lattice) and the step
+                    const unsigned int hnode = sr_node((unsigned int)((t + a.zoff) * plane + cn0.off), a.sr_step);
+                    float vmax = 0.f;
 #pragma unroll
-                for (int f = 0; f < nout; ++f) {
-                    const T st = (sizeof(T) == 2 && a.sr) ? cvt_out_sr<T>(o[f], a, f, sr_field(hnode, f)) : cvt_out<T>(o[f], a, f);
-                    po[f * a.N] = st;
-                    chk += Stor<T>::ld(st);
+                    for (int f = 0; f < nout; f += 2) {
+                        const int g = f + 1 < nout ? f + 1 : f;
+                        vmax = fmaxf(vmax, store_pair16<T>(po, a, f, g, o[f], o[g], a.sr, sr_field(hnode, f)));
+                    }
+                    // non-finite, or beyond the storage's range (NaN fails the comparison)
+                    bad = !(vmax <= Stor16Max<T>::value);
+                } else {
+                    float chk = 0.f;
+#pragma unroll
+                    for (int f = 0; f < nout; ++f) {
+                        po[f * a.N] = o[f];
+                        chk += o[f];
+                    }
+                    bad = !isfinite(chk);
                 }
-                if (!isfinite(chk)) atomicOr(a.flags, 1u);
+                if (bad) atomicOr(a.flags, 1u);
                 }
             }
         }

@@ -1,6 +1,7 @@
 """Long-run effect of the 16-bit moment storage on the channel flow.
 
     python -m entropicthreadsafe_b200.precision_study [--steps 20000] [--every 500] [--avg 5000] [--out result.json]
+    python -m entropicthreadsafe_b200.precision_study --table200 [--out result.json]
 
 The two-component channel (workloads.channel, 384 x 192 x 128, 40 droplets)
 is advanced with the moments stored in FP32, in BF16 and in FP16 with a
@@ -23,6 +24,12 @@ tests/test_gpu_precision.py.  A second FP32 run whose initial velocity is
 perturbed by 1e-6 (relative, uniform noise) measures how far two FP32
 realisations of this droplet-laden flow drift apart by themselves: the
 floor below which a storage form's deviation is not an error of its own.
+
+--table200 measures the short-run errors on the same full channel: each
+storage form (with its stochastic rounding) after 200 steps against the
+FP64 oracle run of the same 200 steps, per moment field as max and L2
+relative error (max|a - b| / max|b|, ||a - b||_2 / ||b||_2; rho as rho - 1).
+The FP64 oracle takes a few minutes on the host cores.
 """
 from __future__ import annotations
 
@@ -97,6 +104,46 @@ def run(precision: int, steps: int, every: int, avg: int, perturb: float = 0.0) 
             "snapshots": len(profs), "mass": red["mass"], "umax": red["umax"]}
 
 
+def field_errors(a: dict, b: dict) -> dict:
+    """Per moment field: (max, L2) relative error of a against b; rho as rho - 1."""
+    from entropicthreadsafe_b200 import capi
+    out = {}
+    for k in capi.FIELDS:
+        x, y = np.asarray(a[k], np.float64), np.asarray(b[k], np.float64)
+        if k == "rho":
+            x, y = x - 1.0, y - 1.0
+        d = x - y
+        out[k] = {"max": float(np.abs(d).max() / max(np.abs(y).max(), 1e-30)),
+                  "l2": float(np.sqrt((d * d).sum() / max((y * y).sum(), 1e-60)))}
+    return out
+
+
+def table200(steps: int = 200) -> dict:
+    """Every storage form on the full channel after `steps` steps against the FP64 oracle."""
+    import oracle
+    from entropicthreadsafe_b200 import capi, workloads
+    from entropicthreadsafe_b200.solver import Lattice
+    p, f = workloads.channel()
+    nz, ny, nx = f["rho"].shape
+    t0 = time.perf_counter()
+    o = oracle.Oracle(p, nx, ny, nz, fp64=True, fast=True)
+    o.set_moments({k: np.asarray(v, np.float64) for k, v in f.items()})
+    o.step(steps)
+    ref = o.get_moments()
+    o.close()
+    res = {"steps": steps, "oracle_seconds": time.perf_counter() - t0, "forms": {}}
+    for name, prec in (("fp32", capi.PREC_FP32), ("bf16", capi.PREC_BF16), ("fp16s", capi.PREC_FP16S)):
+        p.precision = prec
+        with Lattice(p, nx, ny, nz) as lat:
+            lat.upload_moments(f)
+            lat.step(steps)
+            got = lat.download()
+        res["forms"][name] = {"fields": field_errors(got, ref),
+                              "mean_profile_max_rel_err": float(np.abs(mean_profile(got["u"]) - mean_profile(ref["u"])).max()
+                                                                / np.abs(mean_profile(ref["u"])).max())}
+    return res
+
+
 def main(argv=None) -> int:
     from entropicthreadsafe_b200 import capi
     ap = argparse.ArgumentParser()
@@ -104,7 +151,15 @@ def main(argv=None) -> int:
     ap.add_argument("--every", type=int, default=500)
     ap.add_argument("--avg", type=int, default=5000)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--table200", action="store_true", help="200-step errors of every storage form against FP64")
     a = ap.parse_args(argv)
+    if a.table200:
+        res = table200()
+        print(json.dumps(res))
+        if a.out:
+            with open(a.out, "w") as fh:
+                json.dump(res, fh)
+        return 0
     from entropicthreadsafe_b200.solver import TslbError
     res = {"steps": a.steps, "every": a.every, "avg": a.avg}
     runs = {}

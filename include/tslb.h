@@ -350,29 +350,28 @@ int  tslb_ensemble_synchronize(tslb_ensemble* e);
 void* tslb_ensemble_stream(tslb_ensemble* e);
 const char* tslb_ensemble_last_error(tslb_ensemble* e);
 
-/* Largest lattice (nodes) tslb_step_noalloc accepts. */
-#define TSLB_NOALLOC_MAX_NODES (1LL << 20)
+/* Size of tslb_step_noalloc's device scratch (32-bit words). */
+#define TSLB_NOALLOC_SCRATCH_WORDS 64
 
 /* One time step on caller-owned device buffers, allocating nothing.
  *
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc -- a host that owns all device memory itself (an OpenACC data
  * region, a memory pool, a real-time loop that must not allocate).  The
- * scratch the step needs (interface normals of the phase-field mode, the
- * non-finite flag) lives in a fixed device array inside the library, sized
- * for TSLB_NOALLOC_MAX_NODES nodes (12 MB on every GPU that loads the
- * library, held until the process exits); larger lattices are rejected.
+ * only scratch the step needs, its non-finite flag, lives in a fixed device
+ * array inside the library (TSLB_NOALLOC_SCRATCH_WORDS words on every GPU
+ * that loads the library, held until the process exits); it does not grow
+ * with the lattice (the phase-field step forms its interface normals
+ * itself), so the call takes any lattice size the context API takes.
  *
  * d_in and d_out hold the 11 fields in the library's device layout: field
  * f at d_x + f * field_stride (floats), x fastest, field 0 = rho - 1, then
  * u, v, w, pxx, pxy, pxz, pyy, pyz, pzz, phi.  Both 16-byte aligned,
  * field_stride >= nx*ny*nz and a multiple of 4; the two ranges of
- * 11 * field_stride floats must not overlap.  In phase-field mode the
- * normals share the state's field stride inside the scratch, so there
- * field_stride <= TSLB_NOALLOC_MAX_NODES as well.  Inlet faces are not
- * supported (their planes need storage).  The work is queued on `stream`
+ * 11 * field_stride floats must not overlap.  Inlet faces are not supported
+ * (their planes need storage).  The work is queued on `stream`
  * (cudaStream_t, NULL = default stream) and not waited for.  A step that
- * produces a non-finite moment sets a flag in the scratch; read it with
+ * produces a non-finite moment sets the flag; read it with
  * tslb_noalloc_check.
  *
  * The first call on a device (of this function or tslb_noalloc_check)

@@ -78,8 +78,9 @@ def test_driver_droplet_matches_python_path_and_writes_files(tmp_path):
 
 def test_driver_jet_restarts_from_its_dump(tmp_path):
     a, b = tmp_path / "a", tmp_path / "b"
-    run_driver("--workload", "jet", "--n", 32, "--steps", 60, "--stamp", 60, "--dump", 30, "--out", a, "--quiet")
-    run_driver("--workload", "jet", "--n", 32, "--steps", 30, "--stamp", 60, "--out", b, "--quiet",
+    # n = 64: an inlet disc of radius 2.7 nodes (32 would give four nodes)
+    run_driver("--workload", "jet", "--n", 64, "--steps", 60, "--stamp", 60, "--dump", 30, "--out", a, "--quiet")
+    run_driver("--workload", "jet", "--n", 64, "--steps", 30, "--stamp", 60, "--out", b, "--quiet",
                "--load", a / "dump_state_000030.ckpt")
     full = read_vti_data(a / "out_phi_000001.vti")
     restarted = read_vti_data(b / "out_phi_000001.vti")

@@ -78,7 +78,7 @@ def test_device_time_averages():
 def test_closure_study_runs_on_a_shrunk_jet(tmp_path):
     from entropicthreadsafe_b200 import closure_study
     out = tmp_path / "study.json"
-    r = closure_study.main(["--shrink", "8", "--steps", "4000", "--avg-from", "2000", "--snap-every", "400",
+    r = closure_study.main(["--shrink", "8", "--steps", "8000", "--avg-from", "4000", "--snap-every", "800",
                             "--keep-every", "2", "--train-steps", "200", "--batch", "4096", "--fine-seeds", "1", "2",
                             "--train-seeds", "1", "--coarse-seeds", "3", "--check-seeds", "4", "--gains", "1", "2",
                             "--out", str(out)])
@@ -90,6 +90,8 @@ def test_closure_study_runs_on_a_shrunk_jet(tmp_path):
     assert np.isfinite(r["a_priori_held_out"]["loss_net"])
     for run in r["fine_runs"]:
         assert run["diverged_at"] is None and run["gpu_s"] > 0
+        # the averaging window holds the jet: every statistic is a number
+        assert all(np.isfinite(run["stats"][k]) for k in closure_study.SCALARS), run["stats"]
     assert all(d is None for d in r["coarse_plain"]["diverged"])
     for g in ("1.0", "2.0"):
         assert all(d is None for d in r["coarse_closure"][g]["diverged"])

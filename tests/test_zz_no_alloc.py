@@ -3,11 +3,10 @@
 Some hosts cannot let a library call cudaMalloc -- a Fortran driver whose
 device arrays live in an OpenACC data region, a code that hands all GPU
 memory to its own pool, a time loop that must never allocate.  For them
-the library offers one entry point that allocates nothing: its scratch
-(interface normals, the non-finite flag) is a fixed device array inside
-libtslb.so, so lattices are limited to TSLB_NOALLOC_MAX_NODES nodes.
-A step that produces a non-finite moment sets a flag in that array, which
-tslb_noalloc_check reads back (and clears) on the caller's stream.
+the library offers one entry point that allocates nothing: the only
+scratch the step needs, its non-finite flag, is a fixed device array inside
+libtslb.so (TSLB_NOALLOC_SCRATCH_WORDS words), which tslb_noalloc_check
+reads back (and clears) on the caller's stream.
 
 These tests run that entry point twice in a row through the C-ABI and
 compare each result with the context API (tslb_create/tslb_step) on the
@@ -111,25 +110,31 @@ def test_noalloc_colour_matches_context_api_two_calls():
         assert_close(got[k], ref[k], f"colour, call {k + 1}")
 
 
-def test_noalloc_rejects_oversize_and_aliased_buffers():
+def test_noalloc_rejects_aliased_and_short_buffers():
     import torch
     L = capi.lib()
     p = capi.default_params()
     buf = torch.zeros((11, 64), dtype=torch.float32, device="cuda")
     ptr = ctypes.c_void_p(buf.data_ptr())
-    # more nodes than the fixed scratch holds
-    rc = L.tslb_step_noalloc(ctypes.addressof(p), 1024, 1024, 2, ptr, ptr, 64, None)
-    assert rc == capi.ERR_ARG
-    assert b"TSLB_NOALLOC_MAX_NODES" in L.tslb_last_error(None)
-    # input and output must differ
+    # input and output must differ (and not overlap)
     rc = L.tslb_step_noalloc(ctypes.addressof(p), 4, 4, 4, ptr, ptr, 64, None)
     assert rc == capi.ERR_ARG
-    # phase field: a field stride beyond the scratch's normal stride
-    big = torch.zeros((2, 11 * (capi.NOALLOC_MAX_NODES + 64)), dtype=torch.float32, device="cuda")
-    rc = L.tslb_step_noalloc(ctypes.addressof(p), 4, 4, 4, ctypes.c_void_p(big[0].data_ptr()),
-                             ctypes.c_void_p(big[1].data_ptr()), capi.NOALLOC_MAX_NODES + 64, None)
+    assert b"overlap" in L.tslb_last_error(None)
+    # a field stride below the lattice
+    other = torch.zeros((11, 64), dtype=torch.float32, device="cuda")
+    rc = L.tslb_step_noalloc(ctypes.addressof(p), 8, 8, 8, ptr, ctypes.c_void_p(other.data_ptr()), 64, None)
     assert rc == capi.ERR_ARG
     assert b"field_stride" in L.tslb_last_error(None)
+
+
+def test_noalloc_takes_a_lattice_larger_than_any_fixed_scratch():
+    """The scratch does not grow with the lattice: a 128 x 96 x 96 phase-field
+    box (1.2 M nodes) steps like the context API."""
+    p, f = workloads.droplet(n=96, radius=20.0, mode=capi.MODE_PHASEFIELD)
+    big = {k: np.concatenate([v, v[:, :, :32]], axis=2) for k, v in f.items()}   # 128 x 96 x 96
+    ref = context_steps(p, big, 1)
+    got = noalloc_steps(p, big, 1)
+    assert_close(got[0], ref[0], "phase field, 128 x 96 x 96")
 
 
 def test_noalloc_reports_a_non_finite_step_and_allocates_nothing():
