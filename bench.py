@@ -510,6 +510,18 @@ def run_ours(args):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tpn * nodes if tpn else None, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": alg_bytes, "kernel": "tslb::step_kernel<colour>"}
+    # second ceiling: instruction issue.  The kernel executes `ipn` thread
+    # instructions per lattice update (ncu counter smsp__thread_inst_executed.sum
+    # of one launch / its nodes, committed with the traffic figure); an SM
+    # issues at most 4 warp instructions (128 thread instructions) per cycle.
+    ipn = tinfo.get("thread_instructions_per_node") if tinfo else None
+    if ipn and clk and clk.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        issue_rate = sms * 4 * 32 * clk["sm_mhz"] * 1e6          # thread instructions per second
+        lups = nodes / (ms_step * 1e-3)
+        roof["issue"] = {"thread_instructions_per_lu": ipn, "sms": sms, "sm_mhz": clk["sm_mhz"],
+                         "ceiling_mlups": issue_rate / ipn / 1e6, "frac": lups * ipn / issue_rate,
+                         "source": tinfo.get("instructions_command")}
     if rank != 0:
         if ws > 1:
             import torch.distributed as dist
