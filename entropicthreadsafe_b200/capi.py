@@ -104,6 +104,8 @@ def _declare_closure(L) -> None:
         "tslb_closure_destroy": ([vp], None),
         "tslb_closure_set_params": ([vp, fp, fp, fp, ctypes.c_float], ip),
         "tslb_closure_get_params": ([vp, fp, fp, fp, fp], ip),
+        "tslb_closure_set_dtau_min": ([vp, ctypes.c_float], ip),
+        "tslb_closure_dtau_min": ([vp], ctypes.c_float),
         "tslb_closure_forward": ([vp, fp, ll, fp], ip),
         "tslb_closure_gradient": ([vp, fp, fp, fp, ll, fp, dp], ip),
         "tslb_closure_dataset_clear": ([vp], ip),
@@ -223,6 +225,8 @@ def lib() -> ctypes.CDLL:
         L.tslb_stats_accumulate.restype = ip
         L.tslb_stats_download.argtypes = [vp, ip, fp, fp, fp, fp, fp, lp]
         L.tslb_stats_download.restype = ip
+        L.tslb_stats_download_stress.argtypes = [vp, ip, fp, fp, lp]
+        L.tslb_stats_download_stress.restype = ip
         _declare_closure(L)
         cp = ctypes.c_char_p
         for name, args, res in (("tslb_write_raw", [cp, fp, ctypes.c_longlong], ip),

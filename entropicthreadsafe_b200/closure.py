@@ -107,7 +107,12 @@ class Closure:
         sd = np.empty(NFEAT, np.float32)
         dm = ctypes.c_float()
         self._check(self.L.tslb_closure_get_params(self.h, capi.fptr(p), capi.fptr(mu), capi.fptr(sd), ctypes.byref(dm)))
-        return {"params": p, "mu": mu, "sd": sd, "dtau_max": float(dm.value)}
+        return {"params": p, "mu": mu, "sd": sd, "dtau_max": float(dm.value),
+                "dtau_min": float(self.L.tslb_closure_dtau_min(self.h))}
+
+    def set_dtau_min(self, dtau_min: float) -> None:
+        """Lower bound of the output (<= 0): dtau = lo + (hi - lo) sigmoid(o)."""
+        self._check(self.L.tslb_closure_set_dtau_min(self.h, float(dtau_min)))
 
     # -- evaluation ---------------------------------------------------------
     def forward(self, features: np.ndarray) -> np.ndarray:
@@ -187,6 +192,8 @@ def trained_closure(path: str = TRAINED_JET) -> "Closure":
     t = load_trained(path)
     c = Closure()
     c.set_params(t["params"], t["mu"], t["sd"], float(t["dtau_max"]) * float(t["gain"]))
+    if "dtau_min" in t:
+        c.set_dtau_min(float(t["dtau_min"]) * float(t["gain"]))
     return c
 
 

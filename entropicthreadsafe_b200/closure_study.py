@@ -208,6 +208,31 @@ def gain_check(seeds, steps: int = 20000, avg_from: int = 8000, sample_every: in
                 fine_spread=ref["spread"], fine_gpu_s=ref["gpu_s"])
 
 
+def calibrate(seeds, settings, steps: int = 20000, avg_from: int = 8000, sample_every: int = 10, interval: int = 2,
+              ref: dict | None = None) -> dict:
+    """Coarse runs with the packaged network (closure.load_trained) at each
+    (gain, dtau_min) setting: dtau = dtau_min + (gain dtau_max - dtau_min)
+    sigmoid(o).  A tiny gain with a negative dtau_min is the uniform
+    viscosity change alone, the control for what the network adds."""
+    from .closure import load_trained
+    t = load_trained()
+    ref = load_reference() if ref is None else ref
+    out = {}
+    c = Closure()
+    try:
+        for gain, lo in settings:
+            c.set_params(t["params"], t["mu"], t["sd"], float(t["dtau_max"]) * float(gain))
+            c.set_dtau_min(float(lo))
+            runs = [run_jet(1, sd, steps, avg_from, sample_every, {}, closure=c, interval=interval) for sd in seeds]
+            e = _summary(runs, ref)
+            out[f"gain {gain} dtau_min {lo}"] = e
+            print(f"gain {gain}, dtau_min {lo}:", {k: round(v, 4) for k, v in e.get("vs_fine", {}).items()},
+                  {k: round(v, 5) for k, v in e.get("mean", {}).items()}, flush=True)
+    finally:
+        c.close()
+    return out
+
+
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--out", default=None)
@@ -234,7 +259,16 @@ def main(argv=None) -> dict:
                     help="output gains of the a posteriori calibration")
     ap.add_argument("--reference-only", action="store_true",
                     help="only the fine runs: write their reference statistics to --out")
+    ap.add_argument("--calibrate", nargs="*", default=None, metavar="GAIN:DTAU_MIN",
+                    help="only coarse runs of the packaged network at these settings on --coarse-seeds")
     args = ap.parse_args(argv)
+    if args.calibrate is not None:
+        settings = [tuple(float(v) for v in c.split(":")) for c in args.calibrate]
+        r = calibrate(args.coarse_seeds, settings, args.steps, args.avg_from, args.sample_every, args.interval)
+        if args.out:
+            with open(args.out, "w") as fh:
+                json.dump(r, fh, indent=1, default=float)
+        return r
     K = args.shrink
     over = {}
     if K > 1:

@@ -37,7 +37,7 @@ struct tslb_closure {
     float* loss_dev = nullptr;
     int loss_cap = 0;
     unsigned int* flags = nullptr;
-    float mu[NFEAT], sd[NFEAT], dtau_max = 0.01f;
+    float mu[NFEAT], sd[NFEAT], dtau_max = 0.01f, dtau_min = 0.f;
     long long adam_t = 0;
     // training set
     float* ds_feat = nullptr;
@@ -236,7 +236,7 @@ struct LatticeSrc {
     __device__ void store(long long i, float y, float b) const { dtau[i] = y + b; }
 };
 
-// Inference: dtau = dtau_max sigmoid(o) for every row of the source, 128
+// Inference: dtau = dtau_min + (dtau_max - dtau_min) sigmoid(o) for every row of the source, 128
 // rows per tile, tiles strided over a persistent grid.  The next tile's
 // inputs are loaded while this tile's MMAs run; both layers accumulate in
 // the same 64 TMEM columns, so up to 7 CTAs share an SM.
@@ -277,10 +277,10 @@ __global__ void __launch_bounds__(TILE, 6) infer_kernel(const Image* __restrict_
         }
         if (!wait_mma(S.bar, ph, S.abort_s, gflag)) break;
         const float o = epi_out(tb, im, 0);
-        float y = im.dtau_max / (1.f + expf(-o));
+        float y = im.dtau_min + (im.dtau_max - im.dtau_min) / (1.f + expf(-o));
         // stability clamp: the plain tau where anything is not finite
         if (!fin || !isfinite(y)) y = 0.f;
-        y = fminf(fmaxf(y, 0.f), im.dtau_max);
+        y = fminf(fmaxf(y, im.dtau_min), im.dtau_max);
         if (valid) src.store(i, y, kept);
     }
     smem_teardown(S, tb, 64, ph);
@@ -355,11 +355,11 @@ __global__ void __launch_bounds__(TILE, 1) train_kernel(const TrainArgs a) {
         if (!wait_mma(S.bar, ph, S.abort_s, a.flags)) break;
         const float o = epi_out(tb, im);
         const float sg = 1.f / (1.f + expf(-o));
-        const float y = im.dtau_max * sg;
+        const float y = im.dtau_min + (im.dtau_max - im.dtau_min) * sg;
         const float r = valid ? y - tg : 0.f;
         lsum = fmaf(a.inv_batch * wg * r, r, lsum);
-        // dL/do = 2/B a (y - t) dy/do, dy/do = y (1 - sigmoid)
-        const float g = valid ? 2.f * a.inv_batch * wg * r * y * (1.f - sg) : 0.f;
+        // dL/do = 2/B a (y - t) dy/do, dy/do = (dtau_max - dtau_min) sigmoid (1 - sigmoid)
+        const float g = valid ? 2.f * a.inv_batch * wg * r * (y - im.dtau_min) * (1.f - sg) : 0.f;
         db3 += g;
         epi_dz2(tb, S.dz, tid, im, g, dw3);
         sync_for_mma();
@@ -645,6 +645,7 @@ int upload_meta(tslb_closure* c) {
     }
     char* base = reinterpret_cast<char*>(c->img);
     CL_TRY(c, cudaMemcpyAsync(base + offsetof(Image, dtau_max), &c->dtau_max, sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CL_TRY(c, cudaMemcpyAsync(base + offsetof(Image, dtau_min), &c->dtau_min, sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CL_TRY(c, cudaMemcpyAsync(base + offsetof(Image, mu), mu, sizeof(mu), cudaMemcpyHostToDevice, c->stream));
     CL_TRY(c, cudaMemcpyAsync(base + offsetof(Image, isd), isd, sizeof(isd), cudaMemcpyHostToDevice, c->stream));
     CL_TRY(c, cudaStreamSynchronize(c->stream));
@@ -863,6 +864,15 @@ int tslb_closure_get_params(tslb_closure* c, float* params, float* mu, float* sd
     return TSLB_OK;
 }
 
+int tslb_closure_set_dtau_min(tslb_closure* c, float dtau_min) {
+    if (!c) return TSLB_ERR_ARG;
+    if (!(dtau_min <= 0.f) || !std::isfinite(dtau_min)) return cfail(c, TSLB_ERR_ARG, "dtau_min must be finite and <= 0");
+    c->dtau_min = dtau_min;
+    return upload_meta(c);
+}
+
+float tslb_closure_dtau_min(const tslb_closure* c) { return c ? c->dtau_min : 0.f; }
+
 int tslb_closure_forward(tslb_closure* c, const float* features, long long n, float* dtau) {
     if (!c) return TSLB_ERR_ARG;
     if (n < 0 || (n > 0 && (!features || !dtau))) return cfail(c, TSLB_ERR_ARG, "tslb_closure_forward: bad arguments");
@@ -1060,6 +1070,9 @@ int tslb_attach_closure(tslb_ctx* L, tslb_closure* c, int interval) {
         return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: colour mode with FP32 storage only");
     if (c->device != L->device) return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: closure and lattice on different devices");
     if (L->solid_on) return tslb_internal::fail(L, TSLB_ERR_UNSUPPORTED, "tslb_attach_closure: not combined with solid nodes");
+    // a negative correction must leave tau above 1/2 (omega below 2) for either component
+    if (!(std::min(L->p.tau_a, L->p.tau_b) + c->dtau_min > 0.5f))
+        return tslb_internal::fail(L, TSLB_ERR_ARG, "tslb_attach_closure: tau + dtau_min must stay above 1/2");
     int rc = tslb_internal::ensure_dtau(L);
     if (rc) return rc;
     // the first refresh sees the static correction as the previous total

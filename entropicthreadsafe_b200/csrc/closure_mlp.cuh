@@ -53,7 +53,7 @@ struct __align__(128) Image {
                      // column 10 holds b1 (input 10 is a constant 1)
     uint4 w2[512];   // W2, K-major B: chunk (n, kc) at (n/8)*64 + kc*8 + n%8
     float b1[NH], b2[NH], w3[NH];   // w3 holds BF16-rounded values
-    float b3, dtau_max, pad0[2];
+    float b3, dtau_max, dtau_min, pad0;
     float mu[KIN], isd[KIN];
 };
 constexpr int IMG_BYTES = (int)((sizeof(Image) + 127) / 128 * 128);

@@ -414,36 +414,43 @@ __global__ void near_bits_kernel(const unsigned char* __restrict__ isfluid, int 
     near[w] = b;
 }
 
-// running sums of u, v, w, phi and w^2 (time averages of the jet statistics)
+// running sums (time averages of the jet statistics): slots u, v, w, phi,
+// ww, then uu, uv, uw, vv, vw and the six Pi^neq components
+constexpr int NSTATS = 16;
 __global__ void stats_accumulate_kernel(const float* __restrict__ s, long long n, long long N, float* __restrict__ acc) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float w = s[F_W * N + i];
-    acc[i] += s[F_U * N + i];
-    acc[N + i] += s[F_V * N + i];
+    const float u = s[F_U * N + i], v = s[F_V * N + i], w = s[F_W * N + i];
+    acc[i] += u;
+    acc[N + i] += v;
     acc[2 * N + i] += w;
     acc[3 * N + i] += s[F_PHI * N + i];
     acc[4 * N + i] += w * w;
+    acc[5 * N + i] += u * u;
+    acc[6 * N + i] += u * v;
+    acc[7 * N + i] += u * w;
+    acc[8 * N + i] += v * v;
+    acc[9 * N + i] += v * w;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[(10 + k) * N + i] += s[(F_XX + k) * N + i];
 }
 
-// means over cf^3 blocks of the running sums: out[k * nc + j], k = u, v, w, phi, w^2
-__global__ void stats_coarsen_kernel(const float* __restrict__ acc, int nx, int ny, int nz, long long N, int cf,
-                                     float inv, float* __restrict__ out) {
+// means over cf^3 blocks of the running sums k0 .. k0 + nk - 1: out[(k - k0) * nc + j]
+__global__ void stats_coarsen_kernel(const float* __restrict__ acc, int nx, int ny, int nz, long long N, int cf, int k0,
+                                     int nk, float inv, float* __restrict__ out) {
     const int cx = nx / cf, cy = ny / cf, cz = nz / cf;
     const long long nc = (long long)cx * cy * cz;
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= nc) return;
     const int X = (int)(j % cx), Y = (int)((j / cx) % cy), Z = (int)(j / ((long long)cx * cy));
-    float sum[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int dz = 0; dz < cf; ++dz)
-        for (int dy = 0; dy < cf; ++dy)
-            for (int dx = 0; dx < cf; ++dx) {
-                const long long i = (long long)(cf * X + dx) + (long long)nx * ((cf * Y + dy) + (long long)ny * (cf * Z + dz));
-#pragma unroll
-                for (int k = 0; k < 5; ++k) sum[k] += acc[k * N + i];
-            }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) out[k * nc + j] = sum[k] * inv;
+    for (int k = k0; k < k0 + nk; ++k) {
+        float sum = 0.f;
+        for (int dz = 0; dz < cf; ++dz)
+            for (int dy = 0; dy < cf; ++dy)
+                for (int dx = 0; dx < cf; ++dx)
+                    sum += acc[k * N + (long long)(cf * X + dx) + (long long)nx * ((cf * Y + dy) + (long long)ny * (cf * Z + dz))];
+        out[(k - k0) * nc + j] = sum * inv;
+    }
 }
 
 int check_flags(tslb_ctx* c) {
@@ -544,6 +551,44 @@ cudaError_t pool_alloc(void** ptr, size_t bytes, int dev, cudaStream_t st) {
 void pool_free(void* ptr, cudaStream_t st) {
     if (ptr) cudaFreeAsync(ptr, st);
 }
+
+// Page-locked host blocks of the contexts (diagnostics results and ring):
+// cudaHostAlloc and cudaFreeHost take milliseconds, so freed blocks are
+// kept (up to kPinnedKeep bytes, process-wide) and handed out again to
+// requests of the same size.
+std::mutex g_pin_mu;
+std::vector<std::pair<size_t, void*>> g_pin_free;
+size_t g_pin_kept = 0;
+constexpr size_t kPinnedKeep = 64u << 20;
+
+cudaError_t pinned_get(void** p, size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        for (size_t i = 0; i < g_pin_free.size(); ++i)
+            if (g_pin_free[i].first == bytes) {
+                *p = g_pin_free[i].second;
+                g_pin_free.erase(g_pin_free.begin() + (long)i);
+                g_pin_kept -= bytes;
+                return cudaSuccess;
+            }
+    }
+    return cudaHostAlloc(p, bytes, cudaHostAllocPortable);
+}
+
+void pinned_put(void* p, size_t bytes) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        if (g_pin_kept + bytes <= kPinnedKeep) {
+            g_pin_free.emplace_back(bytes, p);
+            g_pin_kept += bytes;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+constexpr size_t kRingBytes = sizeof(double) * RED_PARTS * TSLB_REDUCE_QUEUE;
+constexpr size_t kRedHostBytes = sizeof(double) * RED_PARTS;
 
 int ensure_normals(tslb_ctx* c) {
     if (c->nrm) return TSLB_OK;
@@ -772,26 +817,29 @@ int tslb_create(const tslb_params* p, int nx, int ny, int nz, tslb_ctx** out) {
         return bail(e, "allocation (rho)");
     // the step forms the interface normals it needs itself; the normal field
     // is allocated when tslb_download_normals asks for it
-    // the pool's allocations are ordered on the lattice's stream: complete them for every stream
-    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
-    if ((e = cudaMalloc(&c->flags, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMalloc(flags)");
     {
         int sm_count = 148;
         cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, c->device);
         c->red_blocks = 4 * sm_count;
-        // partials, results, ticket (one more double)
-        const size_t red_bytes = sizeof(double) * ((size_t)c->red_blocks * RED_PARTS + RED_PARTS + 1);
-        if ((e = cudaMalloc(&c->red, red_bytes)) != cudaSuccess) return bail(e, "cudaMalloc(reduce)");
-        if ((e = cudaMemset(c->red, 0, red_bytes)) != cudaSuccess) return bail(e, "cudaMemset(reduce)");
-        if ((e = cudaMallocHost(&c->red_host, sizeof(double) * RED_PARTS)) != cudaSuccess) return bail(e, "cudaMallocHost(reduce)");
+        // reduction partials, results and ticket (one more double), then the
+        // non-finite flag: one pool block, cleared on the stream
+        const size_t red_bytes = (sizeof(double) * ((size_t)c->red_blocks * RED_PARTS + RED_PARTS + 1) + 15) / 16 * 16;
+        if ((e = pool_alloc(reinterpret_cast<void**>(&c->red), red_bytes + 16, c->device, c->stream)) != cudaSuccess)
+            return bail(e, "allocation (reduce)");
+        c->flags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(c->red) + red_bytes);
+        if ((e = cudaMemsetAsync(c->red, 0, red_bytes + 16, c->stream)) != cudaSuccess) return bail(e, "cudaMemsetAsync(reduce)");
+        if ((e = pinned_get(reinterpret_cast<void**>(&c->red_host), kRedHostBytes)) != cudaSuccess)
+            return bail(e, "cudaHostAlloc(reduce)");
     }
-    if ((e = cudaMemset(c->flags, 0, sizeof(unsigned int))) != cudaSuccess) return bail(e, "cudaMemset");
     for (int f = 0; f < 6; ++f) {
         if (p->bc[f] != TSLB_BC_INLET) continue;
         size_t bytes = sizeof(float) * 4 * face_area(c, f);
-        if ((e = cudaMalloc(&c->inlet[f], bytes)) != cudaSuccess) return bail(e, "cudaMalloc(inlet)");
-        if ((e = cudaMemset(c->inlet[f], 0, bytes)) != cudaSuccess) return bail(e, "cudaMemset(inlet)");
+        if ((e = pool_alloc(reinterpret_cast<void**>(&c->inlet[f]), bytes, c->device, c->stream)) != cudaSuccess)
+            return bail(e, "allocation (inlet)");
+        if ((e = cudaMemsetAsync(c->inlet[f], 0, bytes, c->stream)) != cudaSuccess) return bail(e, "cudaMemsetAsync(inlet)");
     }
+    // the pool's allocations and the clears are ordered on the lattice's stream: complete them for every stream
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     c->zchunk = choose_zchunk(step_tiles(nx, ny), nz, sms, kStepBlocksPerSM);
@@ -808,17 +856,16 @@ void tslb_destroy(tslb_ctx* c) {
     pool_free(c->io, c->stream);
     pool_free(c->rho_out, c->stream);
     pool_free(c->nrm, c->stream);
+    pool_free(c->red, c->stream);   // with the flag word
+    for (int f = 0; f < 6; ++f) pool_free(c->inlet[f], c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    cudaFree(c->flags);
-    cudaFree(c->red);
-    cudaFreeHost(c->red_host);
-    cudaFreeHost(c->red_ring);
+    pinned_put(c->red_host, kRedHostBytes);
+    pinned_put(c->red_ring, kRingBytes);
     cudaFree(c->dtau);
     cudaFree(c->dtau_base);
     cudaFree(c->solid);
     cudaFree(c->near);
     cudaFree(c->stats);
-    for (int f = 0; f < 6; ++f) cudaFree(c->inlet[f]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1035,7 +1082,7 @@ int tslb_reduce_async(tslb_ctx* c) {
     if (c->red_queued >= TSLB_REDUCE_QUEUE)
         return fail(c, TSLB_ERR_STATE, "tslb_reduce_async: TSLB_REDUCE_QUEUE results wait; call tslb_reduce_collect");
     if (!c->red_ring)
-        CUDA_TRY(c, cudaMallocHost(&c->red_ring, sizeof(double) * RED_PARTS * TSLB_REDUCE_QUEUE));
+        CUDA_TRY(c, pinned_get(reinterpret_cast<void**>(&c->red_ring), kRingBytes));
     int rc = enqueue_reduce(c, c->red_ring + (size_t)c->red_queued * RED_PARTS);
     if (rc) return rc;
     c->red_queued++;
@@ -1163,8 +1210,8 @@ int tslb_download_tau_correction(tslb_ctx* c, float* dtau) {
 
 int tslb_stats_reset(tslb_ctx* c) {
     if (!c) return TSLB_ERR_ARG;
-    if (!c->stats) CUDA_TRY(c, cudaMalloc(&c->stats, sizeof(float) * 5 * c->N));
-    CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, sizeof(float) * 5 * c->N, c->stream));
+    if (!c->stats) CUDA_TRY(c, cudaMalloc(&c->stats, sizeof(float) * NSTATS * c->N));
+    CUDA_TRY(c, cudaMemsetAsync(c->stats, 0, sizeof(float) * NSTATS * c->N, c->stream));
     c->stats_count = 0;
     return TSLB_OK;
 }
@@ -1186,26 +1233,52 @@ int tslb_stats_accumulate(tslb_ctx* c) {
     return TSLB_OK;
 }
 
-int tslb_stats_download(tslb_ctx* c, int coarsen, float* u, float* v, float* w, float* phi, float* ww, long long* count) {
-    if (!c) return TSLB_ERR_ARG;
+namespace {
+// block means of running-sum slots k0 .. k0 + nk - 1 into the host arrays dst[0 .. nk-1] (NULL: skipped)
+int stats_fetch(tslb_ctx* c, const char* who, int coarsen, int k0, int nk, float* const* dst, long long* count) {
     if (coarsen < 1 || c->nx % coarsen || c->ny % coarsen || c->nz % coarsen)
-        return fail(c, TSLB_ERR_ARG, "tslb_stats_download: coarsening factor must divide the lattice sizes");
+        return fail(c, TSLB_ERR_ARG, std::string(who) + ": coarsening factor must divide the lattice sizes");
     if (count) *count = c->stats_count;
-    if (!c->stats || c->stats_count == 0) return fail(c, TSLB_ERR_STATE, "tslb_stats_download: no accumulated samples");
+    if (!c->stats || c->stats_count == 0) return fail(c, TSLB_ERR_STATE, std::string(who) + ": no accumulated samples");
     const long long nc = c->n / ((long long)coarsen * coarsen * coarsen);
     float* tmp = nullptr;
-    CUDA_TRY(c, cudaMalloc(&tmp, sizeof(float) * 5 * nc));
+    CUDA_TRY(c, cudaMalloc(&tmp, sizeof(float) * nk * nc));
     const float inv = 1.0f / ((float)c->stats_count * coarsen * coarsen * coarsen);
-    stats_coarsen_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(c->stats, c->nx, c->ny, c->nz, c->N, coarsen, inv, tmp);
+    stats_coarsen_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(c->stats, c->nx, c->ny, c->nz, c->N, coarsen,
+                                                                            k0, nk, inv, tmp);
     c->launches++;
     cudaError_t e = cudaGetLastError();
-    float* dst[5] = {u, v, w, phi, ww};
-    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+    for (int k = 0; k < nk && e == cudaSuccess; ++k)
         if (dst[k]) e = cudaMemcpyAsync(dst[k], tmp + k * nc, sizeof(float) * nc, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(tmp);
-    if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string("tslb_stats_download: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(c, TSLB_ERR_CUDA, std::string(who) + ": " + cudaGetErrorString(e));
     return TSLB_OK;
+}
+}  // namespace
+
+int tslb_stats_download(tslb_ctx* c, int coarsen, float* u, float* v, float* w, float* phi, float* ww, long long* count) {
+    if (!c) return TSLB_ERR_ARG;
+    float* const dst[5] = {u, v, w, phi, ww};
+    return stats_fetch(c, "tslb_stats_download", coarsen, 0, 5, dst, count);
+}
+
+int tslb_stats_download_stress(tslb_ctx* c, int coarsen, float* uu, float* pineq, long long* count) {
+    if (!c) return TSLB_ERR_ARG;
+    if (coarsen < 1 || c->nx % coarsen || c->ny % coarsen || c->nz % coarsen)
+        return fail(c, TSLB_ERR_ARG, "tslb_stats_download_stress: coarsening factor must divide the lattice sizes");
+    const long long nc = c->n / ((long long)coarsen * coarsen * coarsen);
+    // uu: (uu, uv, uw, vv, vw, ww) as six consecutive arrays of nc values
+    float* const d1[6] = {uu ? uu : nullptr, uu ? uu + nc : nullptr, uu ? uu + 2 * nc : nullptr,
+                          uu ? uu + 3 * nc : nullptr, uu ? uu + 4 * nc : nullptr, uu ? uu + 5 * nc : nullptr};
+    int rc = stats_fetch(c, "tslb_stats_download_stress", coarsen, 5, 5, d1, count);
+    if (rc) return rc;
+    float* const d2[1] = {uu ? uu + 5 * nc : nullptr};
+    rc = stats_fetch(c, "tslb_stats_download_stress", coarsen, 4, 1, d2, count);
+    if (rc) return rc;
+    float* const d3[6] = {pineq ? pineq : nullptr, pineq ? pineq + nc : nullptr, pineq ? pineq + 2 * nc : nullptr,
+                          pineq ? pineq + 3 * nc : nullptr, pineq ? pineq + 4 * nc : nullptr, pineq ? pineq + 5 * nc : nullptr};
+    return stats_fetch(c, "tslb_stats_download_stress", coarsen, 10, 6, d3, count);
 }
 
 int tslb_synchronize(tslb_ctx* c) {
@@ -1646,6 +1719,14 @@ int ens_build(tslb_ensemble* e) {
             args[par].back().sr = 0;
         }
     }
+    // largest items first (the planes a block marches through, its z chunk plus
+    // the two source planes outside it): the last items of a step are then
+    // the short ones, so the SMs run out of work at about the same time
+    auto planes = [&](const WorkItem& w) {
+        const tslb_ctx* c = e->m[w.dom];
+        return std::min(c->zchunk, c->nz - w.bz * c->zchunk) + 2;
+    };
+    std::stable_sort(work.begin(), work.end(), [&](const WorkItem& a, const WorkItem& b) { return planes(a) > planes(b); });
     ens_drop_graph(e);
     cudaFree(e->d_work);
     for (int par = 0; par < 2; ++par) cudaFree(e->d_args[par]);

@@ -32,23 +32,26 @@ namespace tslb {
 constexpr int NF = 11;
 enum { F_D = 0, F_U, F_V, F_W, F_XX, F_XY, F_XZ, F_YY, F_YZ, F_ZZ, F_PHI };
 
-// Coefficient slots (per node, shared memory), ordered in pairs that the
-// pull always reads together, so each pair is one 8-byte load:
-//   (0, z), (zz, c0)       every source
-//   (x, xx), (xz, xxz), (xzz, c1)   sources with cx != 0
-//   (y, yy), (yz, yyz), (yzz, c2)   sources with cy != 0
-//   (xy, xyz), (xxy, xyy)           sources with cx != 0 and cy != 0
-//   (c3, c4)                        every source (c4: the rest population's)
+// Coefficient slots (per node, shared memory), in five quads and one pair
+// that the pull reads whole, so a source reads a quad with one 16-byte load:
+//   q0 (0, z | zz, c0)        every source
+//   q1 (x, xx | xz, xxz)      sources with cx != 0
+//   q2 (y, yy | yz, yyz)      sources with cy != 0
+//   q3 (xzz, c1 | yzz, c2)    the first half for cx != 0, the second for cy != 0
+//   q4 (xy, xyz | xxy, xyy)   sources with cx != 0 and cy != 0
+//   p5 (c3, c4)               every source (c4: the rest population's)
 // Colour slots c0..c4: phi, Bx, By, Bz, delta0 | phase field: G0, G1x, G1y, G1z, -.
 enum {
     K_0 = 0, K_Z, K_ZZ, K_C0,
-    K_X, K_XX, K_XZ, K_XXZ, K_XZZ, K_C1,
-    K_Y, K_YY, K_YZ, K_YYZ, K_YZZ, K_C2,
+    K_X, K_XX, K_XZ, K_XXZ,
+    K_Y, K_YY, K_YZ, K_YYZ,
+    K_XZZ, K_C1, K_YZZ, K_C2,
     K_XY, K_XYZ, K_XXY, K_XYY,
     K_C3, K_C4,
     NCOEF
 };
-static_assert(NCOEF % 2 == 0, "coefficient slots come in pairs");
+constexpr int NQUAD = 5;   // quads q0..q4; slots 4 NQUAD.. form the pair p5
+static_assert(NCOEF == 4 * NQUAD + 2, "coefficient slots: five quads and one pair");
 
 // accumulator slots of a target node
 enum { A_RHO = 0, A_JX, A_JY, A_JZ, A_XX, A_XY, A_XZ, A_YY, A_YZ, A_ZZ, A_COL, NACC };

@@ -29,28 +29,52 @@
 
 namespace tslb {
 
-// Coefficients live in shared memory as NCOEF/2 planes of CAREA float2
-// (slot pairs, pair-major): node n's pair p is at float offset
-// p * 2 CAREA + 2 n.  Each source loads the pairs its directions use, one
-// 8-byte load per pair; lanes (consecutive x) read consecutive 8-byte words.
-__device__ __forceinline__ float coef_at(const float* Kn, int slot) {
-    const float2 v = *reinterpret_cast<const float2*>(Kn + (slot >> 1) * (2 * CAREA));
-    return (slot & 1) ? v.y : v.x;
+// Coefficients live in shared memory as NQUAD planes of CAREA float4 and one
+// plane of CAREA float2: node n's quad q is at float offset q * 4 CAREA + 4 n,
+// its pair p5 at PAIR_OFF + 2 n.  A source loads each quad its directions use
+// with one 16-byte load (lanes, consecutive x, read consecutive 16-byte
+// words), or the half of q3 it uses with an 8-byte load.
+constexpr int PAIR_OFF = 4 * NQUAD * CAREA;
+// a node of the coefficient tile: its quad-plane and pair-plane addresses
+struct CNode {
+    const float* q;   // coef + 4 n
+    const float* p;   // coef + PAIR_OFF + 2 n
+    __device__ __forceinline__ CNode at(int dn) const { return CNode{q + 4 * dn, p + 2 * dn}; }
+};
+__device__ __forceinline__ CNode cnode(const float* coef, int n) { return CNode{coef + 4 * n, coef + PAIR_OFF + 2 * n}; }
+__device__ __forceinline__ float comp4(const float4& v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+// slot of node c: HALF reads the half of its quad that holds it (8 bytes)
+template <bool HALF = false>
+__device__ __forceinline__ float coef_at(const CNode& c, int slot) {
+    if (slot >= 4 * NQUAD) {
+        const float2 v = *reinterpret_cast<const float2*>(c.p);
+        return slot & 1 ? v.y : v.x;
+    }
+    const float* b = c.q + (slot >> 2) * (4 * CAREA);
+    if (HALF) {
+        const float2 v = *reinterpret_cast<const float2*>(b + (slot & 2));
+        return slot & 1 ? v.y : v.x;
+    }
+    return comp4(*reinterpret_cast<const float4*>(b), slot & 3);
 }
 // (single-component mode leaves the colour slots unset: stored, never read)
 template <int MODE>
-__device__ __forceinline__ void store_coefs(float* dst, const float* K) {
+__device__ __forceinline__ void store_coefs(float* coef, int n, const float* K) {
 #pragma unroll
-    for (int p = 0; p < NCOEF / 2; ++p)
-        *reinterpret_cast<float2*>(dst + p * (2 * CAREA)) = make_float2(K[2 * p], K[2 * p + 1]);
+    for (int q = 0; q < NQUAD; ++q)
+        *reinterpret_cast<float4*>(coef + q * (4 * CAREA) + 4 * n) = make_float4(K[4 * q], K[4 * q + 1], K[4 * q + 2], K[4 * q + 3]);
+    *reinterpret_cast<float2*>(coef + PAIR_OFF + 2 * n) = make_float2(K[4 * NQUAD], K[4 * NQUAD + 1]);
 }
 
 // P' = Q0 + cz Q1 + cz^2 Q2 of the directions (CXv, CYv, cz), cz = -1, 0, 1,
-// of the source whose coefficients start at Kp
+// of the source at coefficient node Kp
 template <int CXv, int CYv>
 struct Src {
-    const float* Kp;
-    __device__ __forceinline__ float L(int slot) const { return coef_at(Kp, slot); }
+    CNode Kp;
+    // q3 is read whole only by sources that use both of its halves
+    __device__ __forceinline__ float L(int slot) const {
+        return (slot >> 2) == 3 && !(CXv && CYv) ? coef_at<true>(Kp, slot) : coef_at<false>(Kp, slot);
+    }
     __device__ __forceinline__ void eval(float& Pm, float& P0, float& Pp) const {
         float q0 = L(K_0);
         if (CXv) q0 += CXv * L(K_X) + L(K_XX);
@@ -75,9 +99,9 @@ struct Src {
 // the factors +-1 are exact, so each lane is the scalar evaluation.
 template <int CYv>
 struct SrcPair {
-    const float* Ka;   // source of cx = +1
-    const float* Kb;   // source of cx = -1
-    __device__ __forceinline__ float2 L(int slot) const { return make_float2(coef_at(Ka, slot), coef_at(Kb, slot)); }
+    Src<1, CYv> A;    // source of cx = +1
+    Src<-1, CYv> B;   // source of cx = -1
+    __device__ __forceinline__ float2 L(int slot) const { return make_float2(A.L(slot), B.L(slot)); }
     __device__ __forceinline__ void eval(float2& Pm, float2& P0, float2& Pp) const {
         const float2 sx = make_float2(1.f, -1.f);
         float2 q0 = __fadd2_rn(L(K_0), __ffma2_rn(sx, L(K_X), L(K_XX)));
@@ -136,15 +160,16 @@ __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float 
     float r = Ex;
     if (CYv) r += CYv > 0 ? Ey : -Ey;
     if (CZv) r += CZv > 0 ? Ez : -Ez;
-    float v = fmaf(wE, ha + hb, wC * hc);
-    v = fmaf(wE * invlen(cE), r, v);
+    // summed in units of wE (wC = 4 wE), one weighting into the accumulator
+    float v = fmaf(wC / wE, hc, ha + hb);
+    v = fmaf(invlen(cE), r, v);
     if (cC) {
         float rc = 0.f;
         if (CYv) rc += CYv > 0 ? By0 : -By0;
         if (CZv) rc += CZv > 0 ? Bz0 : -Bz0;
-        v = fmaf(wC * invlen(cC), rc, v);
+        v = fmaf((wC / wE) * invlen(cC), rc, v);
     }
-    acc[A_COL] += v;
+    acc[A_COL] = fmaf(wE, v, acc[A_COL]);
 }
 
 // All populations that leave the source row y - CYv of plane s and land on
@@ -152,15 +177,15 @@ __device__ __forceinline__ void col_group(float* acc, float ha, float hc, float 
 // points at the column's own node in the coefficient tile; phm, ph0, php
 // are the column's own phi in the three target planes (colour mode).
 template <int MODE, int CYv>
-__device__ __forceinline__ void pull_row(const float* __restrict__ Kc, float* accm, float* acc0, float* accp,
+__device__ __forceinline__ void pull_row(const CNode& Kc, float* accm, float* acc0, float* accp,
                                          float phm, float ph0, float php) {
-    const Src<1, CYv> sa{Kc - 2 * (CYv * CW + 1)};   // source of cx = +1 (x - 1)
-    const Src<0, CYv> sz{Kc - 2 * (CYv * CW)};       // source of cx = 0
-    const Src<-1, CYv> sb{Kc - 2 * (CYv * CW - 1)};  // source of cx = -1 (x + 1)
+    const Src<1, CYv> sa{Kc.at(-(CYv * CW + 1))};   // source of cx = +1 (x - 1)
+    const Src<0, CYv> sz{Kc.at(-(CYv * CW))};       // source of cx = 0
+    const Src<-1, CYv> sb{Kc.at(-(CYv * CW - 1))};  // source of cx = -1 (x + 1)
     float am, a0, ap, cm, c0, cp, bm, b0, bp;
     {
         float2 pm, p0, pp;
-        SrcPair<CYv>{sa.Kp, sb.Kp}.eval(pm, p0, pp);
+        SrcPair<CYv>{sa, sb}.eval(pm, p0, pp);
         am = pm.x; bm = pm.y; a0 = p0.x; b0 = p0.y; ap = pp.x; bp = pp.y;
     }
     sz.eval(cm, c0, cp);
@@ -348,7 +373,7 @@ __device__ void boundary_target_k(const StepArgs& a, const float* Kp, unsigned m
 
 // the same, with the target's coefficients read from the coefficient tile at Kc
 template <int MODE, class T, bool TAU = false, bool SOLID = false>
-__device__ __forceinline__ void boundary_target(const StepArgs& a, const float* __restrict__ Kc, unsigned mask, int x, int y,
+__device__ __forceinline__ void boundary_target(const StepArgs& a, const CNode& Kc, unsigned mask, int x, int y,
                                                 int z, float* acc) {
     float Kp[NCOEF];
 #pragma unroll
@@ -434,8 +459,8 @@ __device__ __forceinline__ void pf_normal(const T* ring, int parea, int z, int p
     if constexpr (std::is_same<T, __half>::value) {
         n[0] *= a.iscale[F_PHI]; n[1] *= a.iscale[F_PHI]; n[2] *= a.iscale[F_PHI];
     }
-    const float den = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) + 1e-9f;
-    n[0] /= den; n[1] /= den; n[2] /= den;
+    const float inv = __frcp_rn(sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) + 1e-9f);
+    n[0] *= inv; n[1] *= inv; n[2] *= inv;
 }
 
 
@@ -455,40 +480,46 @@ __device__ __forceinline__ XYNode xy_node(const StepArgs& a, int gx, int gy, boo
     return n;
 }
 
-// Phase-field curvature -div n at a coefficient node: the isotropic stencil
-// over its 26 neighbours (recursive_2c_TSLB3D.f90:617-627), each neighbour's
-// normal recomputed from the staged phi (pf_normal); a neighbour behind a
-// non-periodic face, or an interior solid one, has n = 0.  z is the source
-// plane (ring index), gz its lattice plane, pi the node's staged offset.
+// Phase-field curvature -div n at the coefficient nodes whose lanes ask for
+// it (need): the isotropic stencil over the node's 26 neighbours
+// (recursive_2c_TSLB3D.f90:617-627), each neighbour's normal recomputed from
+// the staged phi (pf_normal); a neighbour behind a non-periodic face, or an
+// interior solid one, has n = 0.  The warp takes the asking nodes one at a
+// time: lane j < 26 computes neighbour j and a butterfly sums the 26 terms.
+// Every lane of the warp calls it.  z is the source plane (ring index), gz
+// its lattice plane, pi and nd the lane's node (staged offset, coordinates).
+static_assert(TX == 32, "a warp is one tile row: the lane is threadIdx.x");
 template <int SWv, bool SOLID, class T>
-__device__ float pf_curvature(const T* ring, int parea, int z, int pi, const StepArgs& a, const XYNode& nd, int gz,
-                              bool xper, bool yper, bool zper) {
-    float div = 0.f;
-#pragma unroll 1
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int zn = gz + dz;
-        if (!zper && (zn < 0 || zn >= a.nz)) continue;
-#pragma unroll 1
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int yn = nd.gy + dy;
-            if (!yper && (yn < 0 || yn >= a.ny)) continue;
-#pragma unroll 1
-            for (int dx = -1; dx <= 1; ++dx) {
-                if (!dx && !dy && !dz) continue;
-                const int xn = nd.gx + dx;
-                if (!xper && (xn < 0 || xn >= a.nx)) continue;
-                if (SOLID && bit_at(a.solid, nidx(a, wrapi(xn, a.nx), wrapi(yn, a.ny), wrapi(zn, a.nz)))) continue;
-                float n[3];
-                pf_normal<SWv>(ring, parea, z + dz, pi + dy * SWv + dx, a, n);
-                float t = 0.f;
-                if (dx) t += dx * n[0];
-                if (dy) t += dy * n[1];
-                if (dz) t += dz * n[2];
-                div += wclass(dx * dx + dy * dy + dz * dz) * t;
-            }
+__device__ float warp_curvature(bool need, const T* ring, int parea, int z, int pi, const StepArgs& a, const XYNode& nd,
+                                int gz, bool xper, bool yper, bool zper) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x;
+    const int j = lane < 13 ? lane : lane + 1;   // 3 x 3 x 3 index of the neighbour, the centre (13) skipped
+    const int dx = j % 3 - 1, dy = (j / 3) % 3 - 1, dz = j / 9 - 1;
+    const float wj = lane < 26 ? wclass(dx * dx + dy * dy + dz * dz) : 0.f;
+    const int zn = gz + dz;
+    const bool zok = lane < 26 && (zper || (zn >= 0 && zn < a.nz));
+    float mine = 0.f;
+    unsigned pend = __ballot_sync(FULL, need);
+    while (pend) {
+        const int src = __ffs(pend) - 1;
+        pend &= pend - 1;
+        const int spi = __shfl_sync(FULL, pi, src);
+        const int xn = __shfl_sync(FULL, nd.gx, src) + dx;
+        const int yn = __shfl_sync(FULL, nd.gy, src) + dy;
+        bool ok = zok && (xper || (xn >= 0 && xn < a.nx)) && (yper || (yn >= 0 && yn < a.ny));
+        if (SOLID && ok) ok = !bit_at(a.solid, nidx(a, wrapi(xn, a.nx), wrapi(yn, a.ny), wrapi(zn, a.nz)));
+        float t = 0.f;
+        if (ok) {
+            float n[3];
+            pf_normal<SWv>(ring, parea, z + dz, spi + dy * SWv + dx, a, n);
+            t = wj * ((float)dx * n[0] + (float)dy * n[1] + (float)dz * n[2]);
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
+        if (lane == src) mine = -3.f * t;
     }
-    return -3.f * div;
+    return mine;
 }
 
 __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
@@ -514,7 +545,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     using G = Geo<sizeof(T), PHR>;
     constexpr int SW = G::SW, EPC = G::EPC, MAREA = G::MAREA, PAREA = G::PAREA;
     extern __shared__ float4 smem4[];
-    float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NCOEF][CAREA]
+    float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NQUAD quads + pair][CAREA]
     T* mst = reinterpret_cast<T*>(coef_base + 2 * NCOEF * CAREA);     // [2][NMOM][MROWS][SW]
     T* phis = mst + 2 * NMOM * MAREA;                                 // [PRING][PROWS][SW] (not single)
     const T* gin = reinterpret_cast<const T*>(a.in);
@@ -705,7 +736,6 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
 #pragma unroll
                 for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
                 float g[3] = {0.f, 0.f, 0.f};
-                float curv = 0.f;
                 if (MODE == TSLB_MODE_COLOUR) {
                     const T* p0 = phis + (s & (PRING - 1)) * PAREA + pi;
                     const T* pm = phis + ((s - 1) & (PRING - 1)) * PAREA + pi;
@@ -715,25 +745,51 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                     if constexpr (std::is_same<T, __half>::value) {
                         g[0] *= a.iscale[F_PHI]; g[1] *= a.iscale[F_PHI]; g[2] *= a.iscale[F_PHI];
                     }
-                } else if (MODE == TSLB_MODE_PHASEFIELD) {
-                    // the interface normal n = grad phi / (|grad phi| + 1e-9) of the node
-                    // (recursive_2c_TSLB3D.f90:555-571), and where the indicator
-                    // phi (1 - phi) |n|^2 exceeds 0.2, the curvature -div n over the 26
-                    // neighbours' normals, each from the staged phi (:614-629)
-                    m[F_PHI] = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
-                    pf_normal<SW>(phis, PAREA, s, pi, a, g);
-                    const float ind = m[F_PHI] * (1.f - m[F_PHI]) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
-                    if (ind > 0.2f) curv = pf_curvature<SW, SOLID>(phis, PAREA, s, pi, a, nd, gz, xper, yper, zper);
                 } else {
                     m[F_PHI] = 1.f;
                 }
-                node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
+                node_coefs<MODE, TAU>(a, m, g, 0.f, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
-            store_coefs<MODE>(coef + 2 * ci, K);
+            store_coefs<MODE>(coef, ci, K);
+        };
+        // Phase field: the interface normal n = grad phi / (|grad phi| + 1e-9) of
+        // the node (recursive_2c_TSLB3D.f90:555-571) and, where the indicator
+        // phi (1 - phi) |n|^2 exceeds 0.2, the curvature -div n over the 26
+        // neighbours' normals (:614-629), which the whole warp computes
+        // (warp_curvature): every lane calls this, has marks the lanes that own
+        // a node.
+        auto coef_node_pf = [&](const bool has, const XYNode& nd, const int ci, const int mi, const int pi) {
+            const bool live = has && !nd.out && !(SOLID && bit_at(a.solid, (long long)gz * plane + nd.off));
+            float phi = 0.f, g[3] = {0.f, 0.f, 0.f};
+            bool need = false;
+            if (live) {
+                phi = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
+                pf_normal<SW>(phis, PAREA, s, pi, a, g);
+                need = phi * (1.f - phi) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 0.2f;
+            }
+            const float curv = warp_curvature<SW, SOLID>(need, phis, PAREA, s, pi, a, nd, gz, xper, yper, zper);
+            if (!has) return;
+            float K[NCOEF];
+            if (live) {
+                float m[NF];
+#pragma unroll
+                for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
+                m[F_PHI] = phi;
+                node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
+            } else {
+#pragma unroll
+                for (int c = 0; c < NCOEF; ++c) K[c] = 0.f;
+            }
+            store_coefs<MODE>(coef, ci, K);
         };
         if (!zsolid) {
-            coef_node(cn0, ci0, mi0, pi0);
-            if (has_rim) coef_node(cn1, ci1, mi1, pi1);
+            if constexpr (MODE == TSLB_MODE_PHASEFIELD) {
+                coef_node_pf(true, cn0, ci0, mi0, pi0);
+                coef_node_pf(has_rim, cn1, ci1, mi1, pi1);
+            } else {
+                coef_node(cn0, ci0, mi0, pi0);
+                if (has_rim) coef_node(cn1, ci1, mi1, pi1);
+            }
         }
         // VEC: all copies issued so far (moments of s+1, phi of s+2) land before the
         // barrier, which also makes them visible for the next plane's coefficients
@@ -742,7 +798,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         __syncthreads();
         // ---- 2. pull ----
         if (active) {
-            const float* Kc = coef + 2 * ((ty + 1) * CW + (tx + 1));
+            const CNode Kc = cnode(coef, (ty + 1) * CW + (tx + 1));
             float phm = 0.f, ph0 = 0.f, php = 0.f;
             if (MODE == TSLB_MODE_COLOUR) {
                 // own-column phi of the target planes s-1 .. s+1

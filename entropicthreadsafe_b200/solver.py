@@ -141,6 +141,17 @@ class Lattice:
         out["count"] = int(cnt.value)
         return out
 
+    def stats_stress(self, coarsen: int = 1) -> dict:
+        """Means of the products u_a u_b ("uu": uu, uv, uw, vv, vw, ww) and of
+        Pi^neq ("pineq": xx, xy, xz, yy, yz, zz) over the accumulated samples,
+        averaged over coarsen^3 blocks; arrays of shape (6, nz', ny', nx')."""
+        nz, ny, nx = self.shape
+        shp = (6, nz // coarsen, ny // coarsen, nx // coarsen)
+        uu, pi = np.empty(shp, np.float32), np.empty(shp, np.float32)
+        cnt = ctypes.c_longlong()
+        self._check(self.L.tslb_stats_download_stress(self.h, coarsen, capi.fptr(uu), capi.fptr(pi), ctypes.byref(cnt)))
+        return {"uu": uu, "pineq": pi, "count": int(cnt.value)}
+
     # -- time stepping ---------------------------------------------------
     def step(self, nsteps: int = 1) -> None:
         self._check(self.L.tslb_step(self.h, nsteps))

@@ -251,17 +251,23 @@ int  tslb_set_tau_correction(tslb_ctx* ctx, const float* dtau);
  * there is none). */
 int  tslb_download_tau_correction(tslb_ctx* ctx, float* dtau);
 
-/* Time averages on the device: tslb_stats_accumulate adds u, v, w, phi and
- * w^2 of the current state to running sums (asynchronous);
- * tslb_stats_download returns their means over the accumulated samples,
- * averaged over coarsen^3 blocks (coarsen divides nx, ny, nz; outputs have
- * (nx/coarsen)*(ny/coarsen)*(nz/coarsen) values; any pointer may be NULL)
- * and the sample count.  They stand in for the host-side averaging the
- * reference's drivers do on frames written by print_module.f90. */
+/* Time averages on the device: tslb_stats_accumulate adds u, v, w, phi,
+ * the six products u_a u_b and the six Pi^neq components of the current
+ * state to running sums (asynchronous; 16 FP32 fields per node);
+ * tslb_stats_download returns the means of u, v, w, phi and w^2 over the
+ * accumulated samples, averaged over coarsen^3 blocks (coarsen divides nx,
+ * ny, nz; outputs have nc = (nx/coarsen)*(ny/coarsen)*(nz/coarsen) values;
+ * any pointer may be NULL) and the sample count;
+ * tslb_stats_download_stress the means of the products into uu (6 x nc:
+ * uu, uv, uw, vv, vw, ww) and of Pi^neq into pineq (6 x nc: xx, xy, xz, yy,
+ * yz, zz), for Reynolds and viscous stresses.  They stand in for the
+ * host-side averaging the reference's drivers do on frames written by
+ * print_module.f90 (no counterpart in its step). */
 int  tslb_stats_reset(tslb_ctx* ctx);
 int  tslb_stats_accumulate(tslb_ctx* ctx);
 int  tslb_stats_download(tslb_ctx* ctx, int coarsen, float* u, float* v, float* w, float* phi, float* ww,
                          long long* count);
+int  tslb_stats_download_stress(tslb_ctx* ctx, int coarsen, float* uu, float* pineq, long long* count);
 
 /* Wait for all work queued on the context stream. */
 int  tslb_synchronize(tslb_ctx* ctx);

@@ -7,7 +7,7 @@
  * time of a colour-mode lattice with a small network evaluated on the GPU
  * every step (or every `interval` steps):
  *
- *   tau_x = tau(phi_x) + dtau_x,   dtau_x = dtau_max * sigmoid(o_x),
+ *   tau_x = tau(phi_x) + dtau_x,   dtau_x = dtau_min + (dtau_max - dtau_min) sigmoid(o_x),
  *   o = w3 . relu(W2 relu(W1 xn + b1) + b2) + b3,   xn = (f - mu) / sd,
  *
  * with the 10 features f of node x (all from the lattice's own moments):
@@ -22,7 +22,9 @@
  * The dense layers run on the tensor cores (tcgen05, BF16 operands, FP32
  * accumulation in tensor memory); W1, W2, w3 are rounded to BF16, biases
  * stay FP32.  Stability clamp: a node whose features or output are not
- * finite keeps the plain tau (dtau = 0); dtau is clamped to [0, dtau_max].
+ * finite keeps the plain tau (dtau = 0); dtau is clamped to [dtau_min,
+ * dtau_max].  dtau_min is 0 unless set (a negative dtau_min lets the
+ * network lower the viscosity; attaching checks tau + dtau_min > 1/2).
  *
  * Training (tslb_closure_train) runs forward and backward passes on the
  * tensor cores and updates FP32 master weights with Adam.  The loss of a
@@ -73,6 +75,9 @@ void tslb_closure_destroy(tslb_closure* c);
  * Any pointer of set_params may be NULL to keep that part. */
 int  tslb_closure_set_params(tslb_closure* c, const float* params, const float* mu, const float* sd, float dtau_max);
 int  tslb_closure_get_params(tslb_closure* c, float* params, float* mu, float* sd, float* dtau_max);
+/* Lower bound of the output, dtau_min <= 0 (0 after create). */
+int  tslb_closure_set_dtau_min(tslb_closure* c, float dtau_min);
+float tslb_closure_dtau_min(const tslb_closure* c);
 
 /* dtau of n feature rows (host arrays). */
 int  tslb_closure_forward(tslb_closure* c, const float* features, long long n, float* dtau);

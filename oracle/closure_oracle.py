@@ -72,8 +72,8 @@ def normalised_input(F, mu, sd, emulate: bool) -> np.ndarray:
     return (F - np.asarray(mu, np.float64)) / np.asarray(sd, np.float64)
 
 
-def forward(p, mu, sd, dtau_max, F, emulate: bool = True):
-    """dtau = dtau_max sigmoid(o) for feature rows F; returns (y, cache)."""
+def forward(p, mu, sd, dtau_max, F, emulate: bool = True, dtau_min: float = 0.0):
+    """dtau = dtau_min + (dtau_max - dtau_min) sigmoid(o) for feature rows F; returns (y, cache)."""
     w = unpack(p)
     W1, W2, w3, b1 = w["W1"], w["W2"], w["w3"], w["b1"]
     if emulate:
@@ -89,20 +89,20 @@ def forward(p, mu, sd, dtau_max, F, emulate: bool = True):
     h2 = np.where(m2, z2, 0.0)
     o = h2 @ w3 + w["b3"]
     sg = 1.0 / (1.0 + np.exp(-o))
-    y = dtau_max * sg
+    y = dtau_min + (dtau_max - dtau_min) * sg
     cache = dict(x=x, m1=m1, h1=h1, m2=m2, h2=h2, sg=sg, W2=W2, w3=w3, o=o)
     return y, cache
 
 
-def loss_and_grad(p, mu, sd, dtau_max, F, t, a, emulate: bool = True):
+def loss_and_grad(p, mu, sd, dtau_max, F, t, a, emulate: bool = True, dtau_min: float = 0.0):
     """Mean of a (y - t)^2 and its gradient with respect to the parameter vector."""
-    y, c = forward(p, mu, sd, dtau_max, F, emulate)
+    y, c = forward(p, mu, sd, dtau_max, F, emulate, dtau_min)
     t = np.asarray(t, np.float64).reshape(-1)
     a = np.asarray(a, np.float64).reshape(-1)
     B = y.shape[0]
     r = y - t
     loss = float(np.sum(a * r * r) / B)
-    g = 2.0 / B * a * r * y * (1.0 - c["sg"])
+    g = 2.0 / B * a * r * (y - dtau_min) * (1.0 - c["sg"])
     dw3 = c["h2"].T @ g
     db3 = g.sum()
     dz2 = g[:, None] * c["w3"][None, :] * c["m2"]

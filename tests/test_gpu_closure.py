@@ -89,6 +89,43 @@ def test_forward_clamps_non_finite_rows():
     assert np.all(np.isfinite(y)) and np.all((y >= 0) & (y <= dm))
 
 
+def test_signed_range_matches_oracle():
+    """A negative lower bound: dtau = lo + (hi - lo) sigmoid(o), forward and
+    gradient against the oracle, outputs inside [lo, hi], non-finite rows
+    at 0; attaching checks that tau + lo stays above 1/2."""
+    p, mu, sd, dm, F, t, a = random_case(4, 640)
+    lo = -0.4 * dm
+    t = (t - 0.5 * dm).astype(np.float32)
+    F[3, 1] = np.nan
+    with closure_with(p, mu, sd, dm) as c:
+        c.set_dtau_min(lo)
+        assert c.get_params()["dtau_min"] == np.float32(lo)
+        y = c.forward(F)
+        g, loss = c.gradient(F, t, a)
+        lat = Lattice(jet_params(tau=0.5 - lo / 2), 16, 16, 16)
+        with pytest.raises(Exception):
+            lattice_attach(lat, c)
+        lat.close()
+    ref, _ = co.forward(p, mu, sd, dm, F, emulate=True, dtau_min=lo)
+    # rows with a non-finite feature keep the plain tau in the kernel (the
+    # oracle's ReLU would map the NaN to 0): compared apart
+    keep = np.isfinite(F).all(axis=1)
+    err = np.abs(y[keep].astype(np.float64) - ref[keep])
+    assert y[3] == 0.0
+    assert np.median(err) <= 1e-5 * (dm - lo) and err.max() <= 2e-3 * (dm - lo), (np.median(err), err.max())
+    assert y.min() >= lo and y.max() <= dm and (y < 0).any()
+    le, ge = co.loss_and_grad(p, mu, sd, dm, F[keep], t[keep], a[keep], emulate=True, dtau_min=lo)
+    with closure_with(p, mu, sd, dm) as c:
+        c.set_dtau_min(lo)
+        g, loss = c.gradient(F[keep], t[keep], a[keep])
+    assert abs(loss - le) <= 1e-4 * le, (loss, le)
+    for name, b0, b1 in BLOCKS:
+        gg, ee = g[b0:b1].astype(np.float64), ge[b0:b1]
+        if name == "W1":
+            gg, ee = (v.reshape(64, 16)[:, :co.NFEAT] for v in (gg, ee))
+        assert np.linalg.norm(gg - ee) <= 2e-3 * np.linalg.norm(ee), name
+
+
 def jet_like_state(nx, ny, nz, seed):
     """A colour state with a droplet, random velocity and stress fields."""
     rng = np.random.default_rng(seed)

@@ -54,6 +54,9 @@ def test_device_time_averages():
         lat.upload_moments(f)
         lat.stats_reset()
         acc = {k: 0.0 for k in ("u", "v", "w", "phi", "ww")}
+        prods = [("u", "u"), ("u", "v"), ("u", "w"), ("v", "v"), ("v", "w"), ("w", "w")]
+        pis = ("pxx", "pxy", "pxz", "pyy", "pyz", "pzz")
+        uu, pi = [0.0] * 6, [0.0] * 6
         for s in range(30):
             if s % spec["refresh"] == 0:
                 workloads.jet_inlet(lat, spec, 3, s)
@@ -64,15 +67,30 @@ def test_device_time_averages():
                 for k in ("u", "v", "w", "phi"):
                     acc[k] = acc[k] + d[k].astype(np.float64)
                 acc["ww"] = acc["ww"] + d["w"].astype(np.float64) ** 2
+                for j, (a, b) in enumerate(prods):
+                    uu[j] = uu[j] + d[a].astype(np.float64) * d[b]
+                for j, k in enumerate(pis):
+                    pi[j] = pi[j] + d[k].astype(np.float64)
         m1 = lat.stats(1)
         m2 = lat.stats(2)
-    assert m1["count"] == 10
-    for k in acc:
-        ref = acc[k] / 10
-        assert np.abs(m1[k] - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1e-3), k
+        s1 = lat.stats_stress(1)
+        s2 = lat.stats_stress(2)
+    assert m1["count"] == 10 and s1["count"] == 10
+    refs = dict(acc)
+    refs.update({f"uu{j}": uu[j] for j in range(6)})
+    refs.update({f"pi{j}": pi[j] for j in range(6)})
+    got1 = dict(m1)
+    got1.update({f"uu{j}": s1["uu"][j] for j in range(6)})
+    got1.update({f"pi{j}": s1["pineq"][j] for j in range(6)})
+    got2 = dict(m2)
+    got2.update({f"uu{j}": s2["uu"][j] for j in range(6)})
+    got2.update({f"pi{j}": s2["pineq"][j] for j in range(6)})
+    for k in refs:
+        ref = refs[k] / 10
+        assert np.abs(got1[k] - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1e-3), k
         nz, ny, nx = ref.shape
         blk = ref.reshape(nz // 2, 2, ny // 2, 2, nx // 2, 2).mean(axis=(1, 3, 5))
-        assert np.abs(m2[k] - blk).max() <= 1e-6 * max(np.abs(blk).max(), 1e-3), k
+        assert np.abs(got2[k] - blk).max() <= 1e-6 * max(np.abs(blk).max(), 1e-3), k
 
 
 def test_closure_study_runs_on_a_shrunk_jet(tmp_path):
