@@ -414,9 +414,13 @@ struct Geo {
 // s+PHR while other threads may still read planes from s-PHR on (the previous
 // iteration's pull or curvature), so the ring holds at least 2 PHR + 1 planes.
 constexpr int PRING = 8;
+// Phase field: the curvature work list of the block (section 4 of step_block):
+// the candidate nodes' tile indices for two planes, their curvatures, two counts
+constexpr size_t CURV_LIST_BYTES = sizeof(float) * CAREA + sizeof(unsigned short) * 2 * CAREA + sizeof(int) * 2;
 __host__ __device__ constexpr size_t step_smem_bytes_es(int mode, int es) {
     return sizeof(float) * 2 * NCOEF * CAREA + (size_t)es * 2 * NMOM * CH * (TX + 2 * (16 / es)) +
-           (mode != TSLB_MODE_SINGLE ? (size_t)es * PRING * (TY + 2 * phi_halo(mode)) * (TX + 2 * (16 / es)) : 0);
+           (mode != TSLB_MODE_SINGLE ? (size_t)es * PRING * (TY + 2 * phi_halo(mode)) * (TX + 2 * (16 / es)) : 0) +
+           (mode == TSLB_MODE_PHASEFIELD ? CURV_LIST_BYTES : 0);
 }
 __host__ __device__ constexpr size_t step_smem_bytes(int mode) { return step_smem_bytes_es(mode, 4); }
 
@@ -480,46 +484,34 @@ __device__ __forceinline__ XYNode xy_node(const StepArgs& a, int gx, int gy, boo
     return n;
 }
 
-// Phase-field curvature -div n at the coefficient nodes whose lanes ask for
-// it (need): the isotropic stencil over the node's 26 neighbours
+// Phase-field curvature -div n of one coefficient node, computed by a whole
+// warp: the isotropic stencil over the node's 26 neighbours
 // (recursive_2c_TSLB3D.f90:617-627), each neighbour's normal recomputed from
 // the staged phi (pf_normal); a neighbour behind a non-periodic face, or an
-// interior solid one, has n = 0.  The warp takes the asking nodes one at a
-// time: lane j < 26 computes neighbour j and a butterfly sums the 26 terms.
-// Every lane of the warp calls it.  z is the source plane (ring index), gz
-// its lattice plane, pi and nd the lane's node (staged offset, coordinates).
+// interior solid one, has n = 0.  Lane j < 26 computes neighbour j and a
+// butterfly sums the 26 terms; every lane returns the sum.  z is the source
+// plane (ring index), gz its lattice plane, pi the node's staged offset and
+// (gx, gy) its lattice coordinates (may lie beyond a periodic face).
 static_assert(TX == 32, "a warp is one tile row: the lane is threadIdx.x");
 template <int SWv, bool SOLID, class T>
-__device__ float warp_curvature(bool need, const T* ring, int parea, int z, int pi, const StepArgs& a, const XYNode& nd,
-                                int gz, bool xper, bool yper, bool zper) {
-    constexpr unsigned FULL = 0xffffffffu;
+__device__ float node_curvature(const T* ring, int parea, int z, int pi, int gx, int gy, int gz, const StepArgs& a,
+                                bool xper, bool yper, bool zper) {
     const int lane = threadIdx.x;
     const int j = lane < 13 ? lane : lane + 1;   // 3 x 3 x 3 index of the neighbour, the centre (13) skipped
     const int dx = j % 3 - 1, dy = (j / 3) % 3 - 1, dz = j / 9 - 1;
-    const float wj = lane < 26 ? wclass(dx * dx + dy * dy + dz * dz) : 0.f;
-    const int zn = gz + dz;
-    const bool zok = lane < 26 && (zper || (zn >= 0 && zn < a.nz));
-    float mine = 0.f;
-    unsigned pend = __ballot_sync(FULL, need);
-    while (pend) {
-        const int src = __ffs(pend) - 1;
-        pend &= pend - 1;
-        const int spi = __shfl_sync(FULL, pi, src);
-        const int xn = __shfl_sync(FULL, nd.gx, src) + dx;
-        const int yn = __shfl_sync(FULL, nd.gy, src) + dy;
-        bool ok = zok && (xper || (xn >= 0 && xn < a.nx)) && (yper || (yn >= 0 && yn < a.ny));
-        if (SOLID && ok) ok = !bit_at(a.solid, nidx(a, wrapi(xn, a.nx), wrapi(yn, a.ny), wrapi(zn, a.nz)));
-        float t = 0.f;
-        if (ok) {
-            float n[3];
-            pf_normal<SWv>(ring, parea, z + dz, spi + dy * SWv + dx, a, n);
-            t = wj * ((float)dx * n[0] + (float)dy * n[1] + (float)dz * n[2]);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
-        if (lane == src) mine = -3.f * t;
+    const int xn = gx + dx, yn = gy + dy, zn = gz + dz;
+    bool ok = lane < 26 && (zper || (zn >= 0 && zn < a.nz)) && (xper || (xn >= 0 && xn < a.nx)) &&
+              (yper || (yn >= 0 && yn < a.ny));
+    if (SOLID && ok) ok = !bit_at(a.solid, nidx(a, wrapi(xn, a.nx), wrapi(yn, a.ny), wrapi(zn, a.nz)));
+    float t = 0.f;
+    if (ok) {
+        float n[3];
+        pf_normal<SWv>(ring, parea, z + dz, pi + dy * SWv + dx, a, n);
+        t = wclass(dx * dx + dy * dy + dz * dz) * ((float)dx * n[0] + (float)dy * n[1] + (float)dz * n[2]);
     }
-    return mine;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return -3.f * t;
 }
 
 __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
@@ -548,6 +540,10 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     float* coef_base = reinterpret_cast<float*>(smem4);               // [2][NQUAD quads + pair][CAREA]
     T* mst = reinterpret_cast<T*>(coef_base + 2 * NCOEF * CAREA);     // [2][NMOM][MROWS][SW]
     T* phis = mst + 2 * NMOM * MAREA;                                 // [PRING][PROWS][SW] (not single)
+    // phase field: curvature work list (curvatures of plane s, candidates of planes s and s+1, their counts)
+    float* cq_curv = reinterpret_cast<float*>(phis + PRING * PAREA);  // [CAREA]
+    unsigned short* cq_list = reinterpret_cast<unsigned short*>(cq_curv + CAREA);   // [2][CAREA]
+    int* cq_n = reinterpret_cast<int*>(cq_list + 2 * CAREA);          // [2]
     const T* gin = reinterpret_cast<const T*>(a.in);
     T* gout = reinterpret_cast<T*>(a.out);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -701,8 +697,37 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         for (int z = z0 - PHR; z <= z0 + PHR - 2; ++z) stage_phi(z);
     stage_mom(z0 - 1);
     cp_async_commit();
+    if (MODE == TSLB_MODE_PHASEFIELD && tid == 0) cq_n[0] = cq_n[1] = 0;
     cp_async_wait<0>();
     __syncthreads();
+
+    // Phase field: the curvature of a plane's interface nodes is shared by all
+    // warps of the block.  The coefficient phase of plane s lists the nodes of
+    // plane s+1 that may need it (candidates: phi (1 - phi) above the
+    // indicator's threshold, a superset of the nodes where phi (1 - phi) |n|^2
+    // exceeds it); the next coefficient phase, after the plane barrier, first
+    // computes their curvatures warp by warp, then (one more barrier) the
+    // coefficients.  A node's position in its plane's list: slot0 / slot1.
+    int slot0 = -1, slot1 = -1;
+    auto list_candidates = [&](int z) {
+        bool zs;
+        const int gzc = zwrap(z, zs);
+        if (zs) { slot0 = slot1 = -1; return; }
+        auto cand = [&](const bool has, const XYNode& nd, const int ci, const int pi) {
+            if (!has || nd.out || (SOLID && bit_at(a.solid, (long long)gzc * plane + nd.off))) return -1;
+            const float ph = cvt_in<T>(phis[(z & (PRING - 1)) * PAREA + pi], a, F_PHI);
+            if (!(ph * (1.f - ph) > 0.2f * (1.f - 1e-5f))) return -1;
+            const int e = atomicAdd(&cq_n[z & 1], 1);
+            cq_list[(z & 1) * CAREA + e] = (unsigned short)ci;
+            return e;
+        };
+        slot0 = cand(true, cn0, ci0, pi0);
+        slot1 = cand(has_rim, cn1, ci1, pi1);
+    };
+    if (MODE == TSLB_MODE_PHASEFIELD) {
+        list_candidates(z0 - 1);
+        __syncthreads();
+    }
 
     float accm[NACC], acc0[NACC], accp[NACC];
 #pragma unroll
@@ -755,41 +780,57 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         // Phase field: the interface normal n = grad phi / (|grad phi| + 1e-9) of
         // the node (recursive_2c_TSLB3D.f90:555-571) and, where the indicator
         // phi (1 - phi) |n|^2 exceeds 0.2, the curvature -div n over the 26
-        // neighbours' normals (:614-629), which the whole warp computes
-        // (warp_curvature): every lane calls this, has marks the lanes that own
-        // a node.
-        auto coef_node_pf = [&](const bool has, const XYNode& nd, const int ci, const int mi, const int pi) {
-            const bool live = has && !nd.out && !(SOLID && bit_at(a.solid, (long long)gz * plane + nd.off));
-            float phi = 0.f, g[3] = {0.f, 0.f, 0.f};
-            bool need = false;
-            if (live) {
-                phi = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
-                pf_normal<SW>(phis, PAREA, s, pi, a, g);
-                need = phi * (1.f - phi) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 0.2f;
-            }
-            const float curv = warp_curvature<SW, SOLID>(need, phis, PAREA, s, pi, a, nd, gz, xper, yper, zper);
-            if (!has) return;
+        // neighbours' normals (:614-629), taken from the block's work list.
+        auto coef_node_pf = [&](const XYNode& nd, const int ci, const int mi, const int pi, const int slot) {
             float K[NCOEF];
-            if (live) {
-                float m[NF];
-#pragma unroll
-                for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
-                m[F_PHI] = phi;
-                node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
-            } else {
+            if (nd.out || (SOLID && bit_at(a.solid, (long long)gz * plane + nd.off))) {
 #pragma unroll
                 for (int c = 0; c < NCOEF; ++c) K[c] = 0.f;
+            } else {
+                float m[NF], g[3];
+#pragma unroll
+                for (int f = 0; f < NMOM; ++f) m[f] = cvt_in<T>(ms[f * MAREA + mi], a, f);
+                const float phi = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
+                m[F_PHI] = phi;
+                pf_normal<SW>(phis, PAREA, s, pi, a, g);
+                const bool need = phi * (1.f - phi) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 0.2f;
+                // a node that needs the curvature was listed as a candidate (slot >= 0)
+                const float curv = need && slot >= 0 ? cq_curv[slot] : 0.f;
+                node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs<MODE>(coef, ci, K);
         };
+        if (MODE == TSLB_MODE_PHASEFIELD) {
+            // curvatures of this plane's candidates, warp w taking entries w, w + 8, ...
+            // (the count is the same for every thread: the list was completed before
+            // the previous plane's barrier)
+            const int cnt = cq_n[s & 1];
+            if (cnt > 0) {
+                for (int e = ty; e < cnt; e += TY) {
+                    const int ci = cq_list[(s & 1) * CAREA + e];
+                    const int cx = ci % CW, cy = ci / CW;
+                    const float k = node_curvature<SW, SOLID>(phis, PAREA, s, cy * SW + cx + G::OFF + (PHR - 1) * SW,
+                                                              x0 - 1 + cx, y0 - 1 + cy, gz, a, xper, yper, zper);
+                    if (tx == 0) cq_curv[e] = k;
+                }
+                __syncthreads();
+                // every thread has read cnt; the next entries of this parity come after the plane barrier
+                if (tid == 0) cq_n[s & 1] = 0;
+            }
+        }
         if (!zsolid) {
             if constexpr (MODE == TSLB_MODE_PHASEFIELD) {
-                coef_node_pf(true, cn0, ci0, mi0, pi0);
-                coef_node_pf(has_rim, cn1, ci1, mi1, pi1);
+                coef_node_pf(cn0, ci0, mi0, pi0, slot0);
+                if (has_rim) coef_node_pf(cn1, ci1, mi1, pi1, slot1);
             } else {
                 coef_node(cn0, ci0, mi0, pi0);
                 if (has_rim) coef_node(cn1, ci1, mi1, pi1);
             }
+        }
+        // phase field: candidates of the next source plane (its phi is staged)
+        if (MODE == TSLB_MODE_PHASEFIELD) {
+            if (more) list_candidates(s + 1);
+            else slot0 = slot1 = -1;
         }
         // VEC: all copies issued so far (moments of s+1, phi of s+2) land before the
         // barrier, which also makes them visible for the next plane's coefficients
