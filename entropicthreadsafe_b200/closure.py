@@ -179,10 +179,11 @@ TRAINED_JET = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "
 
 
 def load_trained(path: str = TRAINED_JET) -> dict:
-    """A trained network: params, mu, sd, dtau_max and the calibrated output
-    gain.  The packaged file is the network of the round-jet study
-    (closure_study: trained on box-filtered 384 x 384 x 768 runs, gain chosen
-    a posteriori on coarse 192 x 192 x 384 runs)."""
+    """A trained network: params, mu, sd, dtau_max, the calibrated output
+    gain and (optional) the output's lower bound dtau_min.  The packaged file
+    is the network of the round-jet study (closure_study: trained on
+    box-filtered 384 x 384 x 768 runs; gain 1 and dtau_min = -0.0007 chosen a
+    posteriori on coarse 192 x 192 x 384 runs, closure_study --calibrate)."""
     d = np.load(path)
     return {k: d[k] for k in d.files}
 

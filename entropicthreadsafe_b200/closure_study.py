@@ -193,7 +193,7 @@ def load_reference(path: str = REFERENCE) -> dict:
 def gain_check(seeds, steps: int = 20000, avg_from: int = 8000, sample_every: int = 10, interval: int = 2,
                ref: dict | None = None) -> dict:
     """Coarse plain and coarse + the trained closure (closure.trained_closure,
-    its calibrated gain included) on the given inlet-noise seeds, against
+    its calibrated gain and lower bound included) on the given inlet-noise seeds, against
     the stored fine reference: the seed means' relative errors of the four
     statistics and the profiles, and the GPU time of each form."""
     from .closure import trained_closure
