@@ -35,23 +35,26 @@ def random_net(seed, dtau_max=0.02):
     return p, mu, sd, dtau_max, F, t, a
 
 
-def test_oracle_backward_matches_finite_differences():
+@pytest.mark.parametrize("lo", [0.0, -0.008])
+def test_oracle_backward_matches_finite_differences(lo):
+    """With and without a negative lower bound of the output (dtau_min)."""
     p, mu, sd, dm, F, t, a = random_net(7)
-    _, g = co.loss_and_grad(p, mu, sd, dm, F, t, a, emulate=False)
+    t = t + lo / 2
+    _, g = co.loss_and_grad(p, mu, sd, dm, F, t, a, emulate=False, dtau_min=lo)
     rng = np.random.default_rng(1)
     # every block of the parameter vector, a few entries each (W1 padding excluded)
     picks = []
-    for name, lo, hi in (("W1", 0, 1024), ("b1", 1024, 1088), ("W2", 1088, 5184), ("b2", 5184, 5248),
+    for name, b0, b1 in (("W1", 0, 1024), ("b1", 1024, 1088), ("W2", 1088, 5184), ("b2", 5184, 5248),
                          ("w3", 5248, 5312), ("b3", 5312, 5313)):
-        cand = [i for i in range(lo, hi) if not (name == "W1" and i % 16 >= co.NFEAT)]
+        cand = [i for i in range(b0, b1) if not (name == "W1" and i % 16 >= co.NFEAT)]
         picks += list(rng.choice(cand, size=min(6, len(cand)), replace=False))
     for i in picks:
         h = 1e-6 * max(1.0, abs(p[i]))
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        lp, _ = co.loss_and_grad(pp, mu, sd, dm, F, t, a, emulate=False)
-        lm, _ = co.loss_and_grad(pm, mu, sd, dm, F, t, a, emulate=False)
+        lp, _ = co.loss_and_grad(pp, mu, sd, dm, F, t, a, emulate=False, dtau_min=lo)
+        lm, _ = co.loss_and_grad(pm, mu, sd, dm, F, t, a, emulate=False, dtau_min=lo)
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(abs(fd), 1e-9) + 1e-12, (i, fd, g[i])
     assert np.all(g[0:1024].reshape(64, 16)[:, co.NFEAT:] == 0.0)
