@@ -522,6 +522,12 @@ def run_ours(args):
         roof["issue"] = {"thread_instructions_per_lu": ipn, "sms": sms, "sm_mhz": clk["sm_mhz"],
                          "ceiling_mlups": issue_rate / ipn / 1e6, "frac": lups * ipn / issue_rate,
                          "source": tinfo.get("instructions_command")}
+        # and the FP32 share: FADD + 2 FFMA + FMUL per update against 128 FP32 lanes per SM, FMA = 2 flops
+        fpn = tinfo.get("fp32_flops_per_node")
+        if fpn:
+            fp32_peak = sms * 128 * 2 * clk["sm_mhz"] * 1e6
+            roof["fp32"] = {"flops_per_lu": fpn, "achieved_tflops": lups * fpn / 1e12,
+                            "peak_tflops": fp32_peak / 1e12, "frac": lups * fpn / fp32_peak}
     if rank != 0:
         if ws > 1:
             import torch.distributed as dist
