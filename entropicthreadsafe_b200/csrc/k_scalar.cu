@@ -50,15 +50,15 @@ cudaError_t scalar_step(const tslb::StepArgs& a, int mode, int prec, cudaStream_
 }
 
 cudaError_t scalar_ensemble(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,
-                            int prec, bool vec, cudaStream_t st, bool launch) {
+                            int prec, bool vec, unsigned int* step, cudaStream_t st, bool launch) {
     using namespace tslb;
     cudaError_t err = cudaSuccess;
     with_storage(prec, [&](auto tag) {
         using T = decltype(tag);
         const size_t sm = step_smem_bytes_es(mode, (int)sizeof(T));
-        auto go = [&](void (*kernel)(const StepArgs*, const WorkItem*, int)) {
+        auto go = [&](void (*kernel)(const StepArgs*, const WorkItem*, int, unsigned int*)) {
             err = ensure_smem_attr((const void*)kernel, sm);
-            if (err == cudaSuccess && launch) kernel<<<grid, dim3(TX, TY, 1), sm, st>>>(args, work, nwork);
+            if (err == cudaSuccess && launch) kernel<<<grid, dim3(TX, TY, 1), sm, st>>>(args, work, nwork, step);
         };
         if (mode == TSLB_MODE_COLOUR) go(vec ? ensemble_kernel<TSLB_MODE_COLOUR, true, T> : ensemble_kernel<TSLB_MODE_COLOUR, false, T>);
         else go(vec ? ensemble_kernel<TSLB_MODE_PHASEFIELD, true, T> : ensemble_kernel<TSLB_MODE_PHASEFIELD, false, T>);

@@ -17,6 +17,6 @@ cudaError_t ensure_smem_attr(const void* fn, size_t bytes);
 // tau correction and interior solid mask
 cudaError_t scalar_step(const tslb::StepArgs& a, int mode, int prec, cudaStream_t st, bool launch);
 cudaError_t scalar_ensemble(const tslb::StepArgs* args, const tslb::WorkItem* work, int nwork, int grid, int mode,
-                            int prec, bool vec, cudaStream_t st, bool launch);
+                            int prec, bool vec, unsigned int* step, cudaStream_t st, bool launch);
 
 }  // namespace tslb_launch

@@ -110,6 +110,7 @@ StepArgs make_args(tslb_ctx* c, const void* in, void* out) {
     a.near = c->solid_on ? c->near : nullptr;
     a.sr = 1;
     a.sr_step = (unsigned int)c->steps_done;
+    a.sr_counter = nullptr;
     for (int f = 0; f < NF; ++f) {
         a.scale[f] = c->scale[f];
         a.iscale[f] = 1.0f / c->scale[f];
@@ -1673,6 +1674,7 @@ struct tslb_ensemble {
     int grid = 0;                      // 0: one block per work item
     int sms = 148;
     int parity = 0;                    // steps taken mod 2 since the last args upload
+    unsigned int* d_step = nullptr;    // {step counter of the stochastic rounding, launch ticket}
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     std::string err;
@@ -1714,9 +1716,9 @@ int ens_build(tslb_ensemble* e) {
         for (int par = 0; par < 2; ++par) {
             const int cur = c->cur ^ par;
             args[par].push_back(make_args(c, c->state[cur], c->state[cur ^ 1]));
-            // the ensemble replays these arguments every step (CUDA graph): no step
-            // counter to seed stochastic rounding, so 16-bit members round to nearest
-            args[par].back().sr = 0;
+            // the ensemble replays these arguments every step (CUDA graph): the step
+            // that seeds the stochastic rounding comes from the device counter
+            args[par].back().sr_counter = e->d_step;
         }
     }
     // largest items first (the planes a block marches through, its z chunk plus
@@ -1748,7 +1750,8 @@ int ens_build(tslb_ensemble* e) {
 cudaError_t ens_kernel(tslb_ensemble* e, bool launch) {
     const int grid = e->grid > 0 ? std::min(e->grid, e->nwork) : e->nwork;
     const StepArgs* args = e->d_args[e->parity];
-    return tslb_launch::scalar_ensemble(args, e->d_work, e->nwork, grid, e->mode, e->precision, e->vec, e->stream, launch);
+    return tslb_launch::scalar_ensemble(args, e->d_work, e->nwork, grid, e->mode, e->precision, e->vec, e->d_step,
+                                        e->stream, launch);
 }
 
 // one ensemble step on the ensemble stream (no host synchronisation)
@@ -1809,6 +1812,9 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
         if (dims[3 * i] % epc) e->vec = false;
     }
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    // step counter of the stochastic rounding (members start at step 0) and launch ticket
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_step, 2 * sizeof(unsigned int));
+    if (ce == cudaSuccess) ce = cudaMemset(e->d_step, 0, 2 * sizeof(unsigned int));
     if (ce == cudaSuccess) ce = ens_kernel(e, false);
     int dev = 0;
     if (ce == cudaSuccess) ce = cudaGetDevice(&dev);
@@ -1835,6 +1841,7 @@ void tslb_ensemble_destroy(tslb_ensemble* e) {
     ens_drop_graph(e);
     cudaFree(e->d_work);
     for (int par = 0; par < 2; ++par) cudaFree(e->d_args[par]);
+    cudaFree(e->d_step);
     for (tslb_ctx* c : e->m) tslb_destroy(c);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -1935,6 +1942,12 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
         if (ce == cudaSuccess) ce = cudaMemcpy(backup[d], c->state[c->cur], bytes, cudaMemcpyDeviceToDevice);
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
     }
+    // and the rounding's step counter, which the tuning steps advance
+    unsigned int step_backup[2] = {0, 0};
+    {
+        cudaError_t ce = cudaMemcpy(step_backup, e->d_step, sizeof(step_backup), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
+    }
     const int zcands[] = {8, 16, 32, 64, 128, 1 << 20};
     const int gcands[] = {kStepBlocksPerSM * e->sms, 0};
     float best = 1e30f;
@@ -1971,6 +1984,10 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
     for (size_t d = 0; d < e->m.size() && rc == TSLB_OK; ++d) {
         tslb_ctx* c = e->m[d];
         cudaError_t ce = cudaMemcpy(c->state[c->cur], backup[d], (size_t)c->esize * NF * c->N, cudaMemcpyDeviceToDevice);
+        if (ce != cudaSuccess) rc = efail(e, TSLB_ERR_CUDA, std::string("tune restore: ") + cudaGetErrorString(ce));
+    }
+    if (rc == TSLB_OK) {
+        cudaError_t ce = cudaMemcpy(e->d_step, step_backup, sizeof(step_backup), cudaMemcpyHostToDevice);
         if (ce != cudaSuccess) rc = efail(e, TSLB_ERR_CUDA, std::string("tune restore: ") + cudaGetErrorString(ce));
     }
     release();

@@ -101,6 +101,7 @@ struct StepArgs {
     int zoff;               // global index of local plane 0 (a z slab's offset; seeds the rounding)
     int sr;                 // 16-bit storage: store the moments with stochastic rounding
     unsigned int sr_step;   // step counter that seeds the rounding (with the node and the field)
+    const unsigned int* sr_counter;  // ensembles: device step counter read instead of sr_step, or null
 };
 
 // Counter-based uniform in [0, 1) of four integers: the reference's

@@ -556,6 +556,9 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
     const bool yper = a.face[2].kind == TSLB_BC_PERIODIC;
     const bool zper = a.face[4].kind == TSLB_BC_PERIODIC;
     const long long plane = (long long)a.nx * a.ny;
+    // the step that seeds the stochastic rounding of 16-bit stores (an ensemble
+    // advances a device counter after each step: its graph replays fixed arguments)
+    const unsigned int sr_step = a.sr_counter ? *a.sr_counter : a.sr_step;
 
     // faces the column touches (z faces are added per plane)
     unsigned colmask = 0;
@@ -891,7 +894,7 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 if constexpr (sizeof(T) == 2) {
                     // 16-bit storage: two fields per conversion (store_pair16), stochastic
                     // rounding seeded by the node (its index in the whole lattice) and the step
-                    const unsigned int hnode = sr_node((unsigned int)((t + a.zoff) * plane + cn0.off), a.sr_step);
+                    const unsigned int hnode = sr_node((unsigned int)((t + a.zoff) * plane + cn0.off), sr_step);
                     float vmax = 0.f;
 #pragma unroll
                     for (int f = 0; f < nout; f += 2) {
@@ -935,9 +938,13 @@ struct WorkItem {
 // lattices (stride gridDim.x); each item is one tile column and z chunk of
 // one lattice.  The lattice's arguments are staged in shared memory when the
 // block moves to a new lattice.  All lattices share MODE, VEC and T.
+// step[0] is the step counter that seeds the stochastic rounding (every
+// member's arguments point at it), step[1] a ticket: the last block of the
+// launch to finish advances the counter, after every block has read it.
 template <int MODE, bool VEC, class T>
 __global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __restrict__ args,
-                                                          const WorkItem* __restrict__ work, int nwork) {
+                                                          const WorkItem* __restrict__ work, int nwork,
+                                                          unsigned int* step) {
     __shared__ StepArgs sa;
     int cur = -1;
     for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
@@ -953,6 +960,14 @@ __global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __res
         }
         step_block<MODE, VEC, T>(sa, w.bx, w.by, w.bz);
         __syncthreads();
+    }
+    if (step && threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        if (atomicAdd(step + 1, 1u) == gridDim.x - 1) {
+            step[1] = 0;
+            step[0] += 1;
+            __threadfence();
+        }
     }
 }
 

@@ -76,7 +76,8 @@ extern "C" {
 #define TSLB_PREC_BF16        1  /* shifted moments in bf16, collision in fp32       */
 #define TSLB_PREC_FP16S       2  /* shifted moments in fp16 with per-field 2^k scale */
 /* The step stores 16-bit moments with stochastic rounding (seeded by node,
- * field and step counter, reproducible; ensemble members round to nearest). */
+ * field and step counter, reproducible; ensembles count their steps on the
+ * device, so their members round as single lattices do). */
 
 /* ---- face boundary kinds; faces are ordered x-, x+, y-, y+, z-, z+ ---- */
 #define TSLB_BC_PERIODIC      0  /* wrap (mpi_module.f90:2083-2118 exchange_pops_intpbc) */

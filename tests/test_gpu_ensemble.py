@@ -36,6 +36,29 @@ def test_ensemble_equals_single_runs_with_graph_and_tuner():
             assert err < 1e-6, (i, k, err)
 
 
+@pytest.mark.parametrize("prec", [capi.PREC_BF16, capi.PREC_FP16S])
+def test_16bit_ensemble_rounds_like_single_runs(prec):
+    """16-bit members store with stochastic rounding seeded by the ensemble's
+    device step counter, so plain launches, graph replays and a tuning pass
+    (which restores the counter with the state) give the single lattices'
+    results bit for bit."""
+    doms = ensemble.couette_droplets(n=4, seed=11)
+    for d in doms:
+        d["params"].precision = prec
+    with ensemble.Ensemble([d["params"] for d in doms], [d["dims"] for d in doms]) as ens:
+        for i, d in enumerate(doms):
+            ens.upload_moments(i, d["fields"])
+        ens.tune()
+        ens.step(3)
+        ens.step_graph(4)
+        ens.step_graph(4)
+        out = [ens.download(i) for i in range(len(doms))]
+    for i, d in enumerate(doms):
+        ref = alone(d, 11)
+        for k in capi.FIELDS:
+            assert np.array_equal(out[i][k], ref[k]), (i, k, float(np.abs(out[i][k] - ref[k]).max()))
+
+
 def test_ensemble_mixed_shapes_phasefield_and_non_vector_width():
     params, dims, fields = [], [], []
     for n in (20, 24, 18):  # nx % 4 != 0 for 18: the ensemble falls back to scalar staging
