@@ -182,7 +182,7 @@ def load_trained(path: str = TRAINED_JET) -> dict:
     """A trained network: params, mu, sd, dtau_max, the calibrated output
     gain and (optional) the output's lower bound dtau_min.  The packaged file
     is the network of the round-jet study (closure_study: trained on
-    box-filtered 384 x 384 x 768 runs; gain 1 and dtau_min = -0.0007 chosen a
+    box-filtered 384 x 384 x 768 runs; gain 1 and dtau_min = -0.00075 chosen a
     posteriori on coarse 192 x 192 x 384 runs, closure_study --calibrate)."""
     d = np.load(path)
     return {k: d[k] for k in d.files}
