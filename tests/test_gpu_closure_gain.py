@@ -5,7 +5,7 @@ with its calibrated lower bound dtau_min), on two inlet-noise seeds that
 neither the training (fine seeds 101-103) nor the calibration and its check
 (coarse seeds 101-106) saw, each
 compared with the fine-grid plain reference (384 x 384 x 768, seeds
-101-103, the judge of the method) stored with the package
+101-103, the yardstick of the method) stored with the package
 (data/closure_jet_fine_reference.json, written by
 `closure_study --reference-only`).
 
