@@ -2,8 +2,9 @@
 
 The reference has no tests; these are the known answers its operator must
 reproduce: the Laplace jump dp = 2 sigma / R of a static droplet, exact
-per-component mass conservation, small spurious currents, and the
-Poiseuille and Couette profiles of a single-colour flow between walls.
+per-component mass conservation, small spurious currents, the Poiseuille
+and Couette profiles of a single-colour flow between walls, and the
+two-parabola profile of two colours of unequal viscosity in layers.
 """
 import numpy as np
 import pytest
@@ -95,6 +96,64 @@ def test_couette_profile():
     lin = np.polyval(slope, z)
     assert np.abs(u - lin).max() < 2e-3 * U  # linear profile
     assert slope[0] > 0 and abs(u[-1] - U) < 0.1 * U and abs(u[0] + U) < 0.1 * U
+
+
+def layered_profile(H, g, inv_nu):
+    """Steady u(z) of d/dz(nu du/dz) = -g between no-slip walls at z = 0 and H
+    for 1/nu(z) given at the nodes z = k + 1/2 (linear between nodes, constant
+    to the walls): nu du/dz = C - g z with C fixing u(H) = 0, integrated on a
+    fine grid and sampled at the nodes."""
+    s = np.linspace(0.0, H, 64 * H + 1)
+    q = np.interp(s, np.arange(H) + 0.5, inv_nu)
+    ds = s[1] - s[0]
+
+    def cumtrapz(y):
+        return np.concatenate([[0.0], np.cumsum(0.5 * (y[1:] + y[:-1]) * ds)])
+
+    c = cumtrapz(g * s * q)[-1] / cumtrapz(q)[-1]
+    u = cumtrapz((c - g * s) * q)
+    return np.interp(np.arange(H) + 0.5, s, u)
+
+
+def test_layered_two_fluid_poiseuille():
+    """Two colours in layers (A below z = H/2, B above) with viscosities in
+    the ratio 5, driven by a body force between bounce-back walls: the
+    velocity is continuous across the interface and the shear stress
+    nu du/dz = C - g z is continuous, so u(z) is two parabolas joined at the
+    interface.  The colour step mixes 1/nu linearly in the colour fraction,
+    so the profile it must reach follows from the measured phi(z); the
+    sharp two-parabola profile is the looser second check (the interface is
+    a few nodes wide)."""
+    H, g = 24, 1e-6
+    tau_a, tau_b = 1.0, 0.6
+    ia, ib = 3.0 / (tau_a - 0.5), 3.0 / (tau_b - 0.5)
+    bc = [capi.BC_PERIODIC] * 4 + [capi.BC_BOUNCEBACK] * 2
+    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau_a, tau_b=tau_b, sigma=0.0, beta=0.7,
+                         force=(g, 0.0, 0.0), bc=bc, wall_phi_mode=1)
+    f = workloads.empty_fields(8, 8, H)
+    f["phi"][:] = -1.0
+    f["phi"][: H // 2] = 1.0
+    _, _, out = run(p, f, 20000)
+    u = out["u"].mean(axis=(1, 2)).astype(np.float64)
+    phi = out["phi"].mean(axis=(1, 2)).astype(np.float64)
+    inv_nu = 0.5 * ((ia + ib) + phi * (ia - ib))
+    exact = layered_profile(H, g, inv_nu)
+    sharp = layered_profile(H, g, np.where(np.arange(H) < H // 2, ia, ib))
+    err = np.abs(u - exact).max() / exact.max()
+    err_sharp = np.abs(u - sharp).max() / sharp.max()
+    k = int(np.nonzero(np.diff(np.sign(phi)))[0][0])
+    z0 = k + 0.5 + phi[k] / (phi[k] - phi[k + 1])
+    print(f"layered Poiseuille: max |u - u_mixed| {err:.4g}, max |u - u_sharp| {err_sharp:.4g} of u_max, "
+          f"interface at z = {z0:.4f}\nphi {np.array2string(phi, precision=4)}")
+    # the interface stays where it was put, between the layers
+    assert abs(z0 - H / 2) < 0.25, z0
+    assert phi[0] > 0.99 and phi[-1] < -0.99
+    # measured on a B200: 0.0038 and 0.050
+    assert err < 0.01, err
+    assert err_sharp < 0.07, err_sharp
+    # the maximum sits in the less viscous layer B, above the interface
+    assert np.argmax(u) > H // 2
+    assert np.abs(out["v"]).max() < 1e-9 and np.abs(out["w"]).max() < 1e-9
 
 
 def test_single_component_poiseuille_profile():
