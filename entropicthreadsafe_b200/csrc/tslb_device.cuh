@@ -449,20 +449,6 @@ __device__ __forceinline__ float eval_P(const float* K, long long stride, int cx
 }
 
 // accumulate population value f (already weighted) of direction c into acc
-template <int CXv, int CYv, int CZv>
-__device__ __forceinline__ void acc_dir(float* acc, float f) {
-    acc[A_RHO] += f;
-    if (CXv > 0) acc[A_JX] += f; else if (CXv < 0) acc[A_JX] -= f;
-    if (CYv > 0) acc[A_JY] += f; else if (CYv < 0) acc[A_JY] -= f;
-    if (CZv > 0) acc[A_JZ] += f; else if (CZv < 0) acc[A_JZ] -= f;
-    if (CXv) acc[A_XX] += f;
-    if (CYv) acc[A_YY] += f;
-    if (CZv) acc[A_ZZ] += f;
-    if (CXv * CYv > 0) acc[A_XY] += f; else if (CXv * CYv < 0) acc[A_XY] -= f;
-    if (CXv * CZv > 0) acc[A_XZ] += f; else if (CXv * CZv < 0) acc[A_XZ] -= f;
-    if (CYv * CZv > 0) acc[A_YZ] += f; else if (CYv * CZv < 0) acc[A_YZ] -= f;
-}
-
 __device__ __forceinline__ void acc_dir_rt(float* acc, int cx, int cy, int cz, float f) {
     acc[A_RHO] += f;
     acc[A_JX] += cx * f; acc[A_JY] += cy * f; acc[A_JZ] += cz * f;
