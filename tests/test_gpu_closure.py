@@ -184,6 +184,11 @@ def test_dataset_from_fine_lattice_matches_oracle():
         n0 = c.dataset_add_fine(lat, 1.9, keep_every=3)
         n1 = c.dataset_add_fine(lat, 1.9, keep_every=3, z_range=(2, 13))
         feat, tgt, wgt = c.dataset()
+        assert c.dataset_size == n0 + n1
+        c.dataset_clear()
+        assert c.dataset_size == 0 and c.dataset()[0].shape[0] == 0
+        # a cleared set fills again from the start
+        assert c.dataset_add_fine(lat, 1.9, keep_every=3) == n0 and c.dataset_size == n0
     rf, rt, rw = co.fine_samples({k: v.astype(np.float32) for k, v in f.items()}, 1.9, (True, True, False))
     nc = rf.shape[0]
     plane = (nx // 2) * (ny // 2)
