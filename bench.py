@@ -258,6 +258,7 @@ def ensemble_leg(args, ndomains: int = 48):
         for i, d in enumerate(doms):
             ens.upload_moments(i, d["fields"])
         zc, gr = ens.tune()
+        rows = ens.tune_results()
         st = torch.cuda.ExternalStream(ens.stream)
         k = args.steps if args.steps % 2 == 0 else args.steps + 1
         ens.step_graph(k)  # capture + warm-up
@@ -291,7 +292,14 @@ def ensemble_leg(args, ndomains: int = 48):
     ms_seq = (time.perf_counter() - t0) * 1e3 / k
     for lat in lats:
         lat.close()
-    return {"domains": ndomains, "nodes": nodes, "steps": k, "tuned": {"zchunk": zc, "grid": gr},
+    # the tuner's table (4 steps per candidate): best time of each grid form
+    per_item = min((r for r in rows if r["grid"] == 0), key=lambda r: r["ms"])
+    resident = min((r for r in rows if r["grid"] > 0), key=lambda r: r["ms"])
+    tuner = {"candidates": len(rows),
+             "best_one_block_per_item": {"zchunk": per_item["zchunk"], "ms_per_step": per_item["ms"]},
+             "best_resident_grid": {"zchunk": resident["zchunk"], "grid": resident["grid"],
+                                    "ms_per_step": resident["ms"]}}
+    return {"domains": ndomains, "nodes": nodes, "steps": k, "tuned": {"zchunk": zc, "grid": gr}, "tuner": tuner,
             "value_graph": nodes / (ms_graph * 1e-3) / 1e6, "value_launch_per_step": nodes / (ms_plain * 1e-3) / 1e6,
             "value_one_at_a_time": nodes / (ms_seq * 1e-3) / 1e6, "unit": UNIT,
             "speedup_vs_one_at_a_time": ms_seq / ms_graph}

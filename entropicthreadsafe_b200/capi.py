@@ -200,6 +200,11 @@ def lib() -> ctypes.CDLL:
         L.tslb_ensemble_reduce.restype = ip
         L.tslb_ensemble_tune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.tslb_ensemble_tune.restype = ip
+        ipp = ctypes.POINTER(ctypes.c_int)
+        L.tslb_ensemble_tune_results.argtypes = [vp, ip, ipp, ipp, ipp, ctypes.POINTER(ctypes.c_float)]
+        L.tslb_ensemble_tune_results.restype = ip
+        L.tslb_ensemble_set_launch.argtypes = [vp, ip, ip]
+        L.tslb_ensemble_set_launch.restype = ip
         L.tslb_ensemble_synchronize.argtypes = [vp]
         L.tslb_ensemble_synchronize.restype = ip
         L.tslb_ensemble_stream.argtypes = [vp]

@@ -1669,6 +1669,8 @@ int tslb_halo_unpack(tslb_ctx* c, int side, const void* d_buf) { return halo_cop
 }  // extern "C"
 
 // ------------------------------------------------------ batched ensemble
+constexpr int kEnsStepWords = 4;   // the ensemble kernel's step counter, ticket and work counter, padded
+
 struct tslb_ensemble {
     std::vector<tslb_ctx*> m;          // member lattices (own state, own params)
     int mode = 0, precision = 0;
@@ -1681,7 +1683,9 @@ struct tslb_ensemble {
     int grid = 0;                      // 0: one block per work item
     int sms = 148;
     int parity = 0;                    // steps taken mod 2 since the last args upload
-    unsigned int* d_step = nullptr;    // {step counter of the stochastic rounding, launch ticket}
+    unsigned int* d_step = nullptr;    // {step counter of the stochastic rounding, launch ticket, work counter, 0}
+    struct TuneRow { int zchunk, grid; float ms; };
+    std::vector<TuneRow> tuned;        // the autotuner's timings, in the order it ran them
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     std::string err;
@@ -1820,8 +1824,8 @@ int tslb_ensemble_create(const tslb_params* params, const int* dims, int n, tslb
     }
     cudaError_t ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     // step counter of the stochastic rounding (members start at step 0) and launch ticket
-    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_step, 2 * sizeof(unsigned int));
-    if (ce == cudaSuccess) ce = cudaMemset(e->d_step, 0, 2 * sizeof(unsigned int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_step, kEnsStepWords * sizeof(unsigned int));
+    if (ce == cudaSuccess) ce = cudaMemset(e->d_step, 0, kEnsStepWords * sizeof(unsigned int));
     if (ce == cudaSuccess) ce = ens_kernel(e, false);
     int dev = 0;
     if (ce == cudaSuccess) ce = cudaGetDevice(&dev);
@@ -1950,7 +1954,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
     }
     // and the rounding's step counter, which the tuning steps advance
-    unsigned int step_backup[2] = {0, 0};
+    unsigned int step_backup[kEnsStepWords] = {0, 0, 0, 0};
     {
         cudaError_t ce = cudaMemcpy(step_backup, e->d_step, sizeof(step_backup), cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
@@ -1963,6 +1967,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     int rc = TSLB_OK;
+    e->tuned.clear();
     for (int zc : zcands) {
         for (int gr : gcands) {
             e->zchunk = zc;
@@ -1979,6 +1984,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
             if (rc) break;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, t0, t1);
+            e->tuned.push_back({zc, gr, ms / reps});
             if (ms < best) { best = ms; bz = zc; bg = gr; }
             // keep the members' buffers consistent with their cur index
             ens_settle(e);
@@ -2006,6 +2012,28 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
     if (zchunk_out) *zchunk_out = bz;
     if (grid_out) *grid_out = bg;
     return TSLB_OK;
+}
+
+int tslb_ensemble_tune_results(tslb_ensemble* e, int max, int* count, int* zchunk, int* grid, float* ms_per_step) {
+    if (!e || !count || max < 0) return TSLB_ERR_ARG;
+    const int n = (int)e->tuned.size();
+    *count = n;
+    for (int i = 0; i < n && i < max; ++i) {
+        if (zchunk) zchunk[i] = e->tuned[i].zchunk;
+        if (grid) grid[i] = e->tuned[i].grid;
+        if (ms_per_step) ms_per_step[i] = e->tuned[i].ms;
+    }
+    return TSLB_OK;
+}
+
+int tslb_ensemble_set_launch(tslb_ensemble* e, int zchunk, int grid) {
+    if (!e) return TSLB_ERR_ARG;
+    if (zchunk < 1 || grid < 0) return efail(e, TSLB_ERR_ARG, "tslb_ensemble_set_launch: need zchunk >= 1 and grid >= 0");
+    ECUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    ens_settle(e);
+    e->zchunk = zchunk;
+    e->grid = grid;
+    return ens_build(e);
 }
 
 int tslb_ensemble_synchronize(tslb_ensemble* e) {

@@ -935,19 +935,24 @@ struct WorkItem {
 };
 
 // Ensemble step: blocks walk a list of work items over many independent
-// lattices (stride gridDim.x); each item is one tile column and z chunk of
-// one lattice.  The lattice's arguments are staged in shared memory when the
-// block moves to a new lattice.  All lattices share MODE, VEC and T.
-// step[0] is the step counter that seeds the stochastic rounding (every
-// member's arguments point at it), step[1] a ticket: the last block of the
-// launch to finish advances the counter, after every block has read it.
+// lattices; each item is one tile column and z chunk of one lattice.  Block
+// b starts with item b; later items go, in list order (longest first), to
+// whichever block asks next (a work counter), so a grid smaller than the
+// list balances items of uneven length.  The lattice's arguments are staged
+// in shared memory when the block moves to a new lattice.  All lattices
+// share MODE, VEC and T.  step[0] is the step counter that seeds the
+// stochastic rounding (every member's arguments point at it), step[1] a
+// ticket and step[2] the work counter: the last block of the launch to
+// finish, after every block has read the step and taken its last item,
+// advances the step and clears the other two for the next launch.
 template <int MODE, bool VEC, class T>
 __global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __restrict__ args,
                                                           const WorkItem* __restrict__ work, int nwork,
                                                           unsigned int* step) {
     __shared__ StepArgs sa;
+    __shared__ int next;
     int cur = -1;
-    for (int it = blockIdx.x; it < nwork; it += gridDim.x) {
+    for (int it = blockIdx.x; it < nwork;) {
         const WorkItem w = work[it];
         if (w.dom != cur) {
             __syncthreads();
@@ -960,11 +965,20 @@ __global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __res
         }
         step_block<MODE, VEC, T>(sa, w.bx, w.by, w.bz);
         __syncthreads();
+        // every thread has read `next` (it was read before this item's barriers)
+        if (step) {
+            if (threadIdx.x == 0 && threadIdx.y == 0) next = (int)gridDim.x + (int)atomicAdd(step + 2, 1u);
+            __syncthreads();
+            it = next;
+        } else {
+            it += gridDim.x;
+        }
     }
     if (step && threadIdx.x == 0 && threadIdx.y == 0) {
         __threadfence();
         if (atomicAdd(step + 1, 1u) == gridDim.x - 1) {
             step[1] = 0;
+            step[2] = 0;
             step[0] += 1;
             __threadfence();
         }

@@ -80,6 +80,22 @@ class Ensemble:
         self._check(self.L.tslb_ensemble_tune(self.h, ctypes.byref(zc), ctypes.byref(gr)))
         return zc.value, gr.value
 
+    def tune_results(self) -> list:
+        """The last tune()'s timings: dicts of zchunk (1 << 20: whole
+        lattices), grid (0: one block per work item) and ms per step."""
+        n = ctypes.c_int()
+        self._check(self.L.tslb_ensemble_tune_results(self.h, 0, ctypes.byref(n), None, None, None))
+        zc = (ctypes.c_int * max(n.value, 1))()
+        gr = (ctypes.c_int * max(n.value, 1))()
+        ms = (ctypes.c_float * max(n.value, 1))()
+        self._check(self.L.tslb_ensemble_tune_results(self.h, n.value, ctypes.byref(n), zc, gr, ms))
+        return [dict(zchunk=zc[i], grid=gr[i], ms=ms[i]) for i in range(n.value)]
+
+    def set_launch(self, zchunk: int, grid: int) -> None:
+        """Fix the z chunk and the grid (0: one block per work item; > 0:
+        that many blocks taking the items as they finish) without tuning."""
+        self._check(self.L.tslb_ensemble_set_launch(self.h, int(zchunk), int(grid)))
+
     def synchronize(self) -> None:
         self._check(self.L.tslb_ensemble_synchronize(self.h))
 

@@ -351,8 +351,17 @@ int  tslb_ensemble_download_moments(tslb_ensemble* e, int i,
                                     float* pyy, float* pyz, float* pzz, float* phi);
 int  tslb_ensemble_reduce(tslb_ensemble* e, int i, double out[TSLB_NREDUCE]);
 /* Autotuner: time the candidate z chunks and grid sizes on the uploaded
- * state (restored afterwards) and keep the fastest; returns the choice. */
+ * state (restored afterwards) and keep the fastest; returns the choice.
+ * grid 0 is one block per work item; grid > 0 that many resident blocks
+ * taking the items in list order (longest first) as they finish. */
 int  tslb_ensemble_tune(tslb_ensemble* e, int* zchunk, int* grid);
+/* The last tuning's timings, in the order they ran: *count rows (at most
+ * max written) of z chunk (1 << 20: whole lattices), grid and milliseconds
+ * per step.  No reference counterpart (the reference has no ensembles). */
+int  tslb_ensemble_tune_results(tslb_ensemble* e, int max, int* count, int* zchunk, int* grid, float* ms_per_step);
+/* Set the z chunk (>= 1) and grid (>= 0, as above) without tuning.  No
+ * reference counterpart. */
+int  tslb_ensemble_set_launch(tslb_ensemble* e, int zchunk, int grid);
 int  tslb_ensemble_synchronize(tslb_ensemble* e);
 void* tslb_ensemble_stream(tslb_ensemble* e);
 const char* tslb_ensemble_last_error(tslb_ensemble* e);

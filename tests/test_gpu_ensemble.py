@@ -25,6 +25,11 @@ def test_ensemble_equals_single_runs_with_graph_and_tuner():
             ens.upload_moments(i, d["fields"])
         zc, gr = ens.tune()
         assert zc > 0
+        # the tuner's table: 6 z chunks x 2 grids, the choice is the fastest row
+        rows = ens.tune_results()
+        assert len(rows) == 12 and all(r["ms"] > 0 for r in rows)
+        best = min(rows, key=lambda r: r["ms"])
+        assert (best["zchunk"], best["grid"]) == (zc, gr)
         ens.step(3)                 # plain launches (odd count)
         ens.step_graph(4)           # graph replay
         ens.step_graph(4)
@@ -49,6 +54,29 @@ def test_16bit_ensemble_rounds_like_single_runs(prec):
         for i, d in enumerate(doms):
             ens.upload_moments(i, d["fields"])
         ens.tune()
+        ens.step(3)
+        ens.step_graph(4)
+        ens.step_graph(4)
+        out = [ens.download(i) for i in range(len(doms))]
+    for i, d in enumerate(doms):
+        ref = alone(d, 11)
+        for k in capi.FIELDS:
+            assert np.array_equal(out[i][k], ref[k]), (i, k, float(np.abs(out[i][k] - ref[k]).max()))
+
+
+@pytest.mark.parametrize("grid", [0, 3, 296], ids=["per_item", "3_blocks", "2_per_sm"])
+def test_every_launch_shape_equals_single_runs(grid):
+    """A fixed z chunk and grid (set_launch): one block per work item, or
+    resident blocks (3: many items each; 296: two per SM) taking the items
+    from the work counter as they finish.  BF16 members, so the rounding's
+    step counter must advance exactly once per launch in every shape."""
+    doms = ensemble.couette_droplets(n=5, seed=13)
+    for d in doms:
+        d["params"].precision = capi.PREC_BF16
+    with ensemble.Ensemble([d["params"] for d in doms], [d["dims"] for d in doms]) as ens:
+        for i, d in enumerate(doms):
+            ens.upload_moments(i, d["fields"])
+        ens.set_launch(16, grid)
         ens.step(3)
         ens.step_graph(4)
         ens.step_graph(4)
