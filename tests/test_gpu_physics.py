@@ -209,9 +209,8 @@ def test_capillary_wave_against_oracle_and_theory():
     tau 0.55) over 6000 steps, about two periods.  Its amplitude history on
     the GPU follows the FP32 oracle's, and its period is within 20% of the
     sharp-interface frequency w0^2 = sigma k^3 / (2 rho): the oracle's own
-    wave is 14% slower at this wavelength and 10% at 128 (the diffuse
-    interface of the colour-gradient model; the gap closes as the wavelength
-    grows), viscosity and amplitude change it by under 1%."""
+    wave is 14% slower at this wavelength and 10% at 128, 17% with the wider
+    interface of beta 0.5; viscosity and amplitude change it by under 1%."""
     import oracle
     nsteps, every = 6000, 50
     p, f = capillary_wave()
