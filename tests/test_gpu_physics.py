@@ -173,22 +173,24 @@ def test_single_component_poiseuille_profile():
     assert np.all(out["phi"] == 1.0)
 
 
-def capillary_wave(nx=64, nz=128, a0=3.0, tau=0.55, sigma=0.01):
-    """Two colours of equal density and viscosity in layers, interface
-    z = nz/2 + a0 cos(2 pi x / nx), walls far above and below."""
+def capillary_wave(mode, nx=64, nz=128, a0=3.0, tau=0.55, sigma=0.01):
+    """Two fluids of equal density and viscosity in layers, interface
+    z = nz/2 + a0 cos(2 pi x / nx), walls far above and below; phi in
+    [-1, 1] (colour) or [0, 1] (phase field, the reference's convention)."""
     bc = [capi.BC_PERIODIC] * 4 + [capi.BC_BOUNCEBACK] * 2
-    p = capi.make_params(mode=capi.MODE_COLOUR, tau_a=tau, tau_b=tau, sigma=sigma, beta=0.7, bc=bc, wall_phi_mode=1)
+    p = capi.make_params(mode=mode, tau_a=tau, tau_b=tau, sigma=sigma, beta=0.7, bc=bc, wall_phi_mode=1)
     f = workloads.empty_fields(nx, 1, nz)
     z = np.arange(nz)[:, None, None] + 0.5
     x = np.arange(nx)[None, None, :]
-    f["phi"][:] = np.tanh((nz / 2 + a0 * np.cos(2 * np.pi * x / nx) - z) / 2.0)
+    th = np.tanh((nz / 2 + a0 * np.cos(2 * np.pi * x / nx) - z) / 2.0)
+    f["phi"][:] = th if mode == capi.MODE_COLOUR else 0.5 * (1.0 + th)
     return p, f
 
 
-def wave_amplitude(phi):
-    """Half the difference of the interface heights (phi = 0, interpolated)
-    at x = 0 and x = nx/2."""
-    ph = np.asarray(phi, np.float64)[:, 0, :]
+def wave_amplitude(phi, level=0.0):
+    """Half the difference of the interface heights (phi = level,
+    interpolated) at x = 0 and x = nx/2."""
+    ph = np.asarray(phi, np.float64)[:, 0, :] - level
     nz, nx = ph.shape
 
     def height(c):
@@ -204,29 +206,33 @@ def wave_period(t, a):
     return 2.0 * float(np.mean(np.diff(zc[1:])))
 
 
-def test_capillary_wave_against_oracle_and_theory():
+@pytest.mark.parametrize("mode,bound", [(capi.MODE_COLOUR, 0.2), (capi.MODE_PHASEFIELD, 0.3)],
+                         ids=["colour", "phasefield"])
+def test_capillary_wave_against_oracle_and_theory(mode, bound):
     """A standing capillary wave (wavelength 64, amplitude 3, sigma 0.01,
     tau 0.55) over 6000 steps, about two periods.  Its amplitude history on
-    the GPU follows the FP32 oracle's, and its period is within 20% of the
-    sharp-interface frequency w0^2 = sigma k^3 / (2 rho): the oracle's own
-    wave is 14% slower at this wavelength and 10% at 128, 17% with the wider
-    interface of beta 0.5; viscosity and amplitude change it by under 1%."""
+    the GPU follows the FP32 oracle's, and its period lies near the
+    sharp-interface period of w0^2 = sigma k^3 / (2 rho).  The oracle's own
+    waves are slower at this resolution: colour 14% (10% at wavelength 128,
+    17% with the wider interface of beta 0.5; viscosity and amplitude change
+    it by under 1%), the reference's phase-field operator 22%."""
     import oracle
     nsteps, every = 6000, 50
-    p, f = capillary_wave()
+    p, f = capillary_wave(mode)
+    level = 0.0 if mode == capi.MODE_COLOUR else 0.5
     nz, _, nx = f["phi"].shape
     t = np.arange(0, nsteps + 1, every, dtype=float)
-    a_gpu, a_ref = [wave_amplitude(f["phi"])], [wave_amplitude(f["phi"])]
+    a_gpu, a_ref = [wave_amplitude(f["phi"], level)], [wave_amplitude(f["phi"], level)]
     with Lattice(p, nx, 1, nz) as lat:
         lat.upload_moments(f)
         for _ in t[1:]:
             lat.step(every)
-            a_gpu.append(wave_amplitude(lat.download()["phi"]))
+            a_gpu.append(wave_amplitude(lat.download()["phi"], level))
     o = oracle.Oracle(p, nx, 1, nz, fp64=False)
     o.set_moments({k: np.asarray(v, np.float64) for k, v in f.items()})
     for _ in t[1:]:
         o.step(every)
-        a_ref.append(wave_amplitude(o.get_moments()["phi"]))
+        a_ref.append(wave_amplitude(o.get_moments()["phi"], level))
     o.close()
     a_gpu, a_ref = np.array(a_gpu), np.array(a_ref)
     k = 2 * np.pi / nx
@@ -236,6 +242,6 @@ def test_capillary_wave_against_oracle_and_theory():
           f"max |a_gpu - a_oracle| {np.abs(a_gpu - a_ref).max():.2e}")
     assert np.abs(a_gpu - a_ref).max() < 0.01 * 3.0
     assert abs(Tg - Tr) < 0.005 * Tr
-    assert abs(Tg / T0 - 1.0) < 0.2
+    assert abs(Tg / T0 - 1.0) < bound
     # damped: the last half period's extremum is below the first's
     assert np.abs(a_gpu[t > nsteps - Tg / 2]).max() < 0.7 * np.abs(a_gpu[(t > Tg / 4) & (t < 3 * Tg / 4)]).max()
