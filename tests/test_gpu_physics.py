@@ -245,3 +245,45 @@ def test_capillary_wave_against_oracle_and_theory(mode, bound):
     assert abs(Tg / T0 - 1.0) < bound
     # damped: the last half period's extremum is below the first's
     assert np.abs(a_gpu[t > nsteps - Tg / 2]).max() < 0.7 * np.abs(a_gpu[(t > Tg / 4) & (t < 3 * Tg / 4)]).max()
+
+
+def test_phasefield_droplet_long_run_agrees_with_oracle():
+    """The reference program's operator (phase field, config 1's kind of
+    droplet: 48^3, R = 12, tau 0.8, sigma 0.01) over 1500 steps, against the
+    reference's FP32 step (the oracle) run alongside: the Laplace jump
+    averaged over steps 750-1500 (it swings with the box's acoustic modes;
+    the operator itself gives about 1.1 x 2 sigma / R), each component's
+    mass and the spurious currents."""
+    import oracle
+    n, R, every, first, last = 48, 12.0, 50, 750, 1500
+    p, f = workloads.droplet(n=n, radius=R, tau=0.8, sigma=0.01, beta=0.7, mode=capi.MODE_PHASEFIELD)
+    names = capi.RED_NAMES
+    gpu, ref = [], []
+    with Lattice(p, n, n, n) as lat:
+        lat.upload_moments(f)
+        g0 = lat.reduce()
+        lat.step(first)
+        for _ in range(first, last, every):
+            lat.step(every)
+            gpu.append(lat.reduce())
+    o = oracle.Oracle(p, n, n, n, fp64=False)
+    o.set_moments({k: np.asarray(v, np.float64) for k, v in f.items()})
+    r0 = dict(zip(names, o.reduce()))
+    o.step(first)
+    for _ in range(first, last, every):
+        o.step(every)
+        ref.append(dict(zip(names, o.reduce())))
+    o.close()
+    lap = 2 * p.sigma / R
+    dg = np.array([r["dp"] for r in gpu]) / lap
+    dr = np.array([r["dp"] for r in ref]) / lap
+    ug = max(r["umax"] for r in gpu)
+    ur = max(r["umax"] for r in ref)
+    drift = {k: ((gpu[-1][k] - g0[k]) / g0[k], (ref[-1][k] - r0[k]) / r0[k]) for k in ("mass", "mass_a", "mass_b")}
+    print(f"phase-field droplet: dp / (2 sigma / R) GPU {dg.mean():.4f}, oracle {dr.mean():.4f}; "
+          f"max sample difference {np.abs(dg - dr).max():.2e}; umax {ug:.3e} / {ur:.3e}; drift {drift}")
+    assert abs(dg.mean() - dr.mean()) < 0.01 * dr.mean()
+    assert 0.9 < dg.mean() < 1.3
+    assert abs(ug - ur) < 0.1 * ur
+    for k, (a, b) in drift.items():
+        assert abs(a) < 1e-4 and abs(a - b) < 5e-5, (k, a, b)
