@@ -316,124 +316,170 @@ __device__ void grad_phi(const StepArgs& a, int x, int y, int z, float g[3]) {
     g[2] = 3.f * gz;
 }
 
-// Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms.
-// m[] are the node's 11 moments (m[F_D] = rho - 1).  gphi: colour mode, the
-// gradient of phi; phase field, the interface normal n, with curv the
-// curvature -div n where the interface indicator exceeds 0.2 (else 0).
-// TAU: the node's relaxation time is tau(phi) + dtau[id] (a local eddy-viscosity
-// correction); the surface-tension coefficient follows the corrected omega.
-template <int MODE, bool TAU = false>
-__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, float curv, float* K,
-                                           long long id = 0) {
-    const float d = m[F_D], rho = 1.f + d;
-    const float u = m[F_U], v = m[F_V], w = m[F_W];
-    const float pxx = m[F_XX], pxy = m[F_XY], pxz = m[F_XZ], pyy = m[F_YY], pyz = m[F_YZ], pzz = m[F_ZZ];
-    const float phi = m[F_PHI];
-    float omega, U, V, W;
-    float A = 0.f, mg = 0.f, nx_ = 0.f, ny_ = 0.f, nz_ = 0.f;
-    bool iface = false;
+// Arithmetic of the coefficient phase, one operation at a time.  The step
+// computes a node's coefficients in every tile whose coefficient tile holds
+// it: as an own node of one tile and as a rim node of its neighbours.  The
+// populations it sends into different tiles must be the same numbers, or
+// mass is not conserved exactly, so no operation is left for the compiler
+// to contract: Ar1 evaluates one node in FP32, Ar2 two nodes at once on the
+// paired FP32 instructions of sm_100 (one node per lane), and both round
+// every operation identically, lane by lane.
+struct Ar1 {
+    using V = float;
+    static __device__ __forceinline__ V c(float x) { return x; }
+    static __device__ __forceinline__ V add(V x, V y) { return __fadd_rn(x, y); }
+    static __device__ __forceinline__ V sub(V x, V y) { return __fsub_rn(x, y); }
+    static __device__ __forceinline__ V mul(V x, V y) { return __fmul_rn(x, y); }
+    static __device__ __forceinline__ V fma(V x, V y, V z) { return __fmaf_rn(x, y, z); }
+    // lane-wise functions (square root, division, selection)
+    template <class F>
+    static __device__ __forceinline__ V map(V x, F f) { return f(x); }
+    template <class F>
+    static __device__ __forceinline__ V map2(V x, V y, F f) { return f(x, y); }
+};
+struct Ar2 {
+    using V = float2;
+    static __device__ __forceinline__ V c(float x) { return make_float2(x, x); }
+    static __device__ __forceinline__ V add(V x, V y) { return __fadd2_rn(x, y); }
+    // x - y rounded once: fma(y, -1, x)
+    static __device__ __forceinline__ V sub(V x, V y) { return __ffma2_rn(y, make_float2(-1.f, -1.f), x); }
+    static __device__ __forceinline__ V mul(V x, V y) { return __fmul2_rn(x, y); }
+    static __device__ __forceinline__ V fma(V x, V y, V z) { return __ffma2_rn(x, y, z); }
+    template <class F>
+    static __device__ __forceinline__ V map(V x, F f) { return make_float2(f(x.x), f(x.y)); }
+    template <class F>
+    static __device__ __forceinline__ V map2(V x, V y, F f) { return make_float2(f(x.x, y.x), f(x.y, y.y)); }
+};
+
+// Per-node coefficients of P'(c) = f_c / w_c - 1 and the colour terms, for
+// one node (Ar1) or two (Ar2).  m[] are the node's 11 moments (m[F_D] =
+// rho - 1).  gphi: colour mode, the gradient of phi; phase field, the
+// interface normal n, with curv the curvature -div n where the interface
+// indicator exceeds 0.2 (else 0).  TAU: the node's relaxation time is
+// tau(phi) + dt (a local eddy-viscosity correction); the surface-tension
+// coefficient follows the corrected omega.
+template <int MODE, bool TAU, class Ar>
+__device__ __forceinline__ void node_coefs_v(const StepArgs& a, const typename Ar::V* m, const typename Ar::V* gphi,
+                                             typename Ar::V curv, typename Ar::V dt, typename Ar::V* K) {
+    using V = typename Ar::V;
+    auto c = [](float x) { return Ar::c(x); };
+    const V d = m[F_D], rho = Ar::add(c(1.f), d);
+    const V u = m[F_U], v = m[F_V], w = m[F_W];
+    const V pxx = m[F_XX], pxy = m[F_XY], pxz = m[F_XZ], pyy = m[F_YY], pyz = m[F_YZ], pzz = m[F_ZZ];
+    const V phi = m[F_PHI];
+    V omega, U, W_, Vv, A = c(0.f), mg = c(0.f), nx_ = c(0.f), ny_ = c(0.f), nz_ = c(0.f);
     if (MODE == TSLB_MODE_COLOUR) {
-        const float* g = gphi;
-        const float m2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-        iface = m2 > a.thr * a.thr;
-        const float rs = rsqrtf(m2);
-        mg = iface ? m2 * rs : 0.f;
+        const V g0 = gphi[0], g1 = gphi[1], g2 = gphi[2];
+        const V m2 = Ar::fma(g2, g2, Ar::fma(g1, g1, Ar::mul(g0, g0)));
+        const float thr2 = a.thr * a.thr;
+        const V rs = Ar::map(m2, [](float x) { return rsqrtf(x); });
+        // branch-free: outside the interface (|g|^2 <= thr^2) A = 0 and n = 0
+        mg = Ar::map2(m2, rs, [thr2](float x, float r) { return x > thr2 ? __fmul_rn(x, r) : 0.f; });
+        const V inv = Ar::map2(m2, rs, [thr2](float x, float r) { return x > thr2 ? r : 0.f; });
         // 1/nu = (rhoA/rho)/nu_a + (rhoB/rho)/nu_b ; omega = 2/(6 nu + 1) = 2q/(6 + q)
-        const float q = 0.5f * ((a.inv_nu_a + a.inv_nu_b) + phi * (a.inv_nu_a - a.inv_nu_b));
-        if (TAU) {
-            // 1/omega = (6 + q)/(2q) + dtau
-            const float dt = __ldg(a.dtau + id);
-            omega = __fdividef(2.f * q, fmaf(2.f * q, dt, 6.f + q));
-        } else {
-            omega = __fdividef(2.f * q, 6.f + q);
-        }
-        // branch-free: outside the interface A = 0 and n = 0
-        const float inv = iface ? rs : 0.f;
-        nx_ = g[0] * inv; ny_ = g[1] * inv; nz_ = g[2] * inv;
-        A = iface ? a.acoef * a.sigma * omega : 0.f;
-        U = u; V = v; W = w;
+        const float qa = 0.5f * (a.inv_nu_a + a.inv_nu_b), qd = 0.5f * (a.inv_nu_a - a.inv_nu_b);
+        const V q = Ar::fma(phi, c(qd), c(qa));
+        const V q2 = Ar::add(q, q);
+        // TAU: 1/omega = (6 + q)/(2q) + dtau
+        const V den = TAU ? Ar::fma(q2, dt, Ar::add(q, c(6.f))) : Ar::add(q, c(6.f));
+        omega = Ar::map2(q2, den, [](float n, float e) { return __fdividef(n, e); });
+        nx_ = Ar::mul(g0, inv); ny_ = Ar::mul(g1, inv); nz_ = Ar::mul(g2, inv);
+        const float acs = a.acoef * a.sigma;
+        A = Ar::map2(m2, omega, [thr2, acs](float x, float o) { return x > thr2 ? __fmul_rn(acs, o) : 0.f; });
+        U = u; Vv = v; W_ = w;
     } else if (MODE == TSLB_MODE_SINGLE) {
         // fused_TSLB_force_1c: equilibrium at the shifted velocity u + F
-        omega = a.omega_pf;
-        U = u + a.force[0];
-        V = v + a.force[1];
-        W = w + a.force[2];
+        omega = c(a.omega_pf);
+        U = Ar::add(u, c(a.force[0]));
+        Vv = Ar::add(v, c(a.force[1]));
+        W_ = Ar::add(w, c(a.force[2]));
     } else {
         // CSF velocity shift u + sigma kappa n (+ F) (recursive_2c_TSLB3D.f90:630-636,
         // lb_kernels_module.f90:769)
-        omega = a.omega_pf;
-        const float n0 = gphi[0], n1 = gphi[1], n2 = gphi[2];
-        const float sk = a.sigma * curv;
-        U = u + sk * n0 + a.force[0];
-        V = v + sk * n1 + a.force[1];
-        W = w + sk * n2 + a.force[2];
-        nx_ = n0; ny_ = n1; nz_ = n2;
+        omega = c(a.omega_pf);
+        const V sk = Ar::mul(c(a.sigma), curv);
+        U = Ar::add(Ar::fma(sk, gphi[0], u), c(a.force[0]));
+        Vv = Ar::add(Ar::fma(sk, gphi[1], v), c(a.force[1]));
+        W_ = Ar::add(Ar::fma(sk, gphi[2], w), c(a.force[2]));
+        nx_ = gphi[0]; ny_ = gphi[1]; nz_ = gphi[2];
     }
-    const float om1 = 1.f - omega;
+    const V om1 = Ar::sub(c(1.f), omega);
     // recursive third-order non-equilibrium moments a3 = u_a Pi_bc + perms
-    const float a_xxy = 2.f * u * pxy + v * pxx;
-    const float a_xxz = 2.f * u * pxz + w * pxx;
-    const float a_xyy = u * pyy + 2.f * v * pxy;
-    const float a_yyz = 2.f * v * pyz + w * pyy;
-    const float a_xzz = u * pzz + 2.f * w * pxz;
-    const float a_yzz = v * pzz + 2.f * w * pyz;
-    const float a_xyz = u * pyz + v * pxz + w * pxy;
-    const float UU = U * U, VV = V * V, WW = W * W;
-    const float rU = rho * U, rV = rho * V, rW = rho * W;
-    // equilibrium third-order moments rho U_a U_b U_c
-    const float e_xxy = rU * U * V, e_xxz = rU * U * W, e_xyy = rU * V * V;
-    const float e_yyz = rV * V * W, e_xzz = rU * W * W, e_yzz = rV * W * W, e_xyz = rU * V * W;
-    const float tr = pxx + pyy + pzz;
-    // full third-order coefficients (eq + (1-omega) neq)
-    const float t_xxy = e_xxy + om1 * a_xxy, t_xxz = e_xxz + om1 * a_xxz, t_xyy = e_xyy + om1 * a_xyy;
-    const float t_yyz = e_yyz + om1 * a_yyz, t_xzz = e_xzz + om1 * a_xzz, t_yzz = e_yzz + om1 * a_yzz;
-    const float t_xyz = e_xyz + om1 * a_xyz;
-    K[K_0] = d - 1.5f * rho * (UU + VV + WW) - 1.5f * om1 * tr;
-    K[K_X] = 3.f * rU - 4.5f * (t_xyy + t_xzz);
-    K[K_Y] = 3.f * rV - 4.5f * (t_xxy + t_yzz);
-    K[K_Z] = 3.f * rW - 4.5f * (t_xxz + t_yyz);
-    K[K_XX] = 4.5f * (rU * U + om1 * pxx);
-    K[K_YY] = 4.5f * (rV * V + om1 * pyy);
-    K[K_ZZ] = 4.5f * (rW * W + om1 * pzz);
-    K[K_XY] = 9.f * (rU * V + om1 * pxy);
-    K[K_XZ] = 9.f * (rU * W + om1 * pxz);
-    K[K_YZ] = 9.f * (rV * W + om1 * pyz);
-    K[K_XXY] = 13.5f * t_xxy;
-    K[K_XXZ] = 13.5f * t_xxz;
-    K[K_XYY] = 13.5f * t_xyy;
-    K[K_YYZ] = 13.5f * t_yyz;
-    K[K_XZZ] = 13.5f * t_xzz;
-    K[K_YZZ] = 13.5f * t_yzz;
-    K[K_XYZ] = 27.f * t_xyz;
+    const V u2 = Ar::add(u, u), v2 = Ar::add(v, v), w2 = Ar::add(w, w);
+    const V a_xxy = Ar::fma(v, pxx, Ar::mul(u2, pxy));
+    const V a_xxz = Ar::fma(w, pxx, Ar::mul(u2, pxz));
+    const V a_xyy = Ar::fma(v2, pxy, Ar::mul(u, pyy));
+    const V a_yyz = Ar::fma(w, pyy, Ar::mul(v2, pyz));
+    const V a_xzz = Ar::fma(w2, pxz, Ar::mul(u, pzz));
+    const V a_yzz = Ar::fma(w2, pyz, Ar::mul(v, pzz));
+    const V a_xyz = Ar::fma(w, pxy, Ar::fma(v, pxz, Ar::mul(u, pyz)));
+    const V rU = Ar::mul(rho, U), rV = Ar::mul(rho, Vv), rW = Ar::mul(rho, W_);
+    // second-order equilibrium products rho U_a U_b
+    const V rUU = Ar::mul(rU, U), rVV = Ar::mul(rV, Vv), rWW = Ar::mul(rW, W_);
+    const V rUV = Ar::mul(rU, Vv), rUW = Ar::mul(rU, W_), rVW = Ar::mul(rV, W_);
+    // full third-order coefficients: rho U_a U_b U_c + (1 - omega) a3
+    const V t_xxy = Ar::fma(om1, a_xxy, Ar::mul(rUU, Vv)), t_xxz = Ar::fma(om1, a_xxz, Ar::mul(rUU, W_));
+    const V t_xyy = Ar::fma(om1, a_xyy, Ar::mul(rUV, Vv)), t_yyz = Ar::fma(om1, a_yyz, Ar::mul(rVV, W_));
+    const V t_xzz = Ar::fma(om1, a_xzz, Ar::mul(rUW, W_)), t_yzz = Ar::fma(om1, a_yzz, Ar::mul(rVW, W_));
+    const V t_xyz = Ar::fma(om1, a_xyz, Ar::mul(rUV, W_));
+    const V tr = Ar::add(Ar::add(pxx, pyy), pzz);
+    // K0 = d - 1.5 (rho |U|^2 + (1 - omega) tr Pi)
+    K[K_0] = Ar::fma(Ar::mul(c(-1.5f), om1), tr, Ar::fma(c(-1.5f), Ar::add(Ar::add(rUU, rVV), rWW), d));
+    K[K_X] = Ar::fma(c(-4.5f), Ar::add(t_xyy, t_xzz), Ar::mul(c(3.f), rU));
+    K[K_Y] = Ar::fma(c(-4.5f), Ar::add(t_xxy, t_yzz), Ar::mul(c(3.f), rV));
+    K[K_Z] = Ar::fma(c(-4.5f), Ar::add(t_xxz, t_yyz), Ar::mul(c(3.f), rW));
+    K[K_XX] = Ar::mul(c(4.5f), Ar::fma(om1, pxx, rUU));
+    K[K_YY] = Ar::mul(c(4.5f), Ar::fma(om1, pyy, rVV));
+    K[K_ZZ] = Ar::mul(c(4.5f), Ar::fma(om1, pzz, rWW));
+    K[K_XY] = Ar::mul(c(9.f), Ar::fma(om1, pxy, rUV));
+    K[K_XZ] = Ar::mul(c(9.f), Ar::fma(om1, pxz, rUW));
+    K[K_YZ] = Ar::mul(c(9.f), Ar::fma(om1, pyz, rVW));
+    K[K_XXY] = Ar::mul(c(13.5f), t_xxy);
+    K[K_XXZ] = Ar::mul(c(13.5f), t_xxz);
+    K[K_XYY] = Ar::mul(c(13.5f), t_xyy);
+    K[K_YYZ] = Ar::mul(c(13.5f), t_yyz);
+    K[K_XZZ] = Ar::mul(c(13.5f), t_xzz);
+    K[K_YZZ] = Ar::mul(c(13.5f), t_yzz);
+    K[K_XYZ] = Ar::mul(c(27.f), t_xyz);
     if (MODE == TSLB_MODE_COLOUR) {
         // force as population source 3 w c.F (recursive_colorTSLB3D.f90:776)
-        K[K_X] += 3.f * a.force[0];
-        K[K_Y] += 3.f * a.force[1];
-        K[K_Z] += 3.f * a.force[2];
+        K[K_X] = Ar::add(K[K_X], c(3.f * a.force[0]));
+        K[K_Y] = Ar::add(K[K_Y], c(3.f * a.force[1]));
+        K[K_Z] = Ar::add(K[K_Z], c(3.f * a.force[2]));
         // perturbation (A/2)|g| [w (c.n)^2 - B_i], B_i = w_i for i >= 1 (A = 0 off the interface)
-        const float h = 0.5f * A * mg;
-        K[K_0] -= h;
-        K[K_XX] += h * nx_ * nx_;
-        K[K_YY] += h * ny_ * ny_;
-        K[K_ZZ] += h * nz_ * nz_;
-        K[K_XY] += 2.f * h * nx_ * ny_;
-        K[K_XZ] += 2.f * h * nx_ * nz_;
-        K[K_YZ] += 2.f * h * ny_ * nz_;
-        const float d0 = (A * (1.f / 3.f)) * mg;  // rest population: B_0 = -10/27 instead of w_0
+        const V h = Ar::mul(Ar::mul(c(0.5f), A), mg), h2 = Ar::add(h, h);
+        K[K_0] = Ar::sub(K[K_0], h);
+        K[K_XX] = Ar::fma(Ar::mul(h, nx_), nx_, K[K_XX]);
+        K[K_YY] = Ar::fma(Ar::mul(h, ny_), ny_, K[K_YY]);
+        K[K_ZZ] = Ar::fma(Ar::mul(h, nz_), nz_, K[K_ZZ]);
+        K[K_XY] = Ar::fma(Ar::mul(h2, nx_), ny_, K[K_XY]);
+        K[K_XZ] = Ar::fma(Ar::mul(h2, nx_), nz_, K[K_XZ]);
+        K[K_YZ] = Ar::fma(Ar::mul(h2, ny_), nz_, K[K_YZ]);
+        // rest population: B_0 = -10/27 instead of w_0
+        const V d0 = Ar::mul(Ar::mul(A, c(1.f / 3.f)), mg);
         // recolouring 2 beta (rhoA rhoB / rho) n  (published form, cos theta; n = 0 off the interface)
-        const float bb = 0.5f * a.beta * rho * (1.f - phi * phi);
-        K[K_C0] = phi; K[K_C1] = bb * nx_; K[K_C2] = bb * ny_; K[K_C3] = bb * nz_; K[K_C4] = d0;
+        const V bb = Ar::mul(Ar::mul(c(0.5f * a.beta), rho), Ar::fma(Ar::mul(c(-1.f), phi), phi, c(1.f)));
+        K[K_C0] = phi; K[K_C1] = Ar::mul(bb, nx_); K[K_C2] = Ar::mul(bb, ny_); K[K_C3] = Ar::mul(bb, nz_); K[K_C4] = d0;
     } else if (MODE == TSLB_MODE_SINGLE) {
-        K[K_C0] = 0.f; K[K_C1] = 0.f; K[K_C2] = 0.f; K[K_C3] = 0.f; K[K_C4] = 0.f;
+        K[K_C0] = c(0.f); K[K_C1] = c(0.f); K[K_C2] = c(0.f); K[K_C3] = c(0.f); K[K_C4] = c(0.f);
     } else if (MODE == TSLB_MODE_PHASEFIELD) {
         // D3Q7 phase field: g_q = G0 + e_q.G1 (recursive_2c_TSLB3D.f90:808-831)
-        const float sh = 0.125f * a.sharp * phi * (1.f - phi);
-        K[K_C0] = 0.125f * phi;
-        K[K_C1] = 0.375f * phi * u + sh * nx_;
-        K[K_C2] = 0.375f * phi * v + sh * ny_;
-        K[K_C3] = 0.375f * phi * w + sh * nz_;
-        K[K_C4] = 0.f;
+        const V sh = Ar::mul(Ar::mul(c(0.125f * a.sharp), phi), Ar::sub(c(1.f), phi));
+        const V p3 = Ar::mul(c(0.375f), phi);
+        K[K_C0] = Ar::mul(c(0.125f), phi);
+        K[K_C1] = Ar::fma(sh, nx_, Ar::mul(p3, u));
+        K[K_C2] = Ar::fma(sh, ny_, Ar::mul(p3, v));
+        K[K_C3] = Ar::fma(sh, nz_, Ar::mul(p3, w));
+        K[K_C4] = c(0.f);
     }
+}
+
+// one node (the call sites of the phase field and of single lattices)
+template <int MODE, bool TAU = false>
+__device__ __forceinline__ void node_coefs(const StepArgs& a, const float* m, const float* gphi, float curv, float* K,
+                                           long long id = 0) {
+    const float dt = TAU ? __ldg(a.dtau + id) : 0.f;
+    node_coefs_v<MODE, TAU, Ar1>(a, m, gphi, curv, dt, K);
 }
 
 // P'(c) for a runtime direction (boundary paths)

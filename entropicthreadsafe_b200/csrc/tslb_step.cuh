@@ -424,36 +424,60 @@ __host__ __device__ constexpr size_t step_smem_bytes_es(int mode, int es) {
 }
 __host__ __device__ constexpr size_t step_smem_bytes(int mode) { return step_smem_bytes_es(mode, 4); }
 
-// gradient 3 sum_i p_i c_i phi(x+c_i) from three phi planes held in shared
-// memory; pm, p0, pp point at the node in planes z-1, z, z+1 (row pitch SWv).
+// gradient 3 sum_i p_i c_i phi(x+c_i) of one node (Ar1) or two (Ar2) from
+// phi planes held in shared memory: P(dz, dx, dy) returns phi at offset
+// (dx, dy, dz) of the node(s).  Every operation is explicit (see Ar1).
+template <class Ar, class LD>
+__device__ __forceinline__ void grad_v(LD P, typename Ar::V g[3]) {
+    using V = typename Ar::V;
+    auto S4 = [](V a, V b, V c, V d) { return Ar::add(Ar::add(Ar::add(a, b), c), d); };
+    const V x1 = Ar::sub(P(0, 1, 0), P(0, -1, 0));
+    const V x2 = Ar::sub(S4(P(0, 1, 1), P(0, 1, -1), P(1, 1, 0), P(-1, 1, 0)),
+                         S4(P(0, -1, 1), P(0, -1, -1), P(1, -1, 0), P(-1, -1, 0)));
+    const V x3 = Ar::sub(S4(P(1, 1, 1), P(1, 1, -1), P(-1, 1, 1), P(-1, 1, -1)),
+                         S4(P(1, -1, 1), P(1, -1, -1), P(-1, -1, 1), P(-1, -1, -1)));
+    const V y1 = Ar::sub(P(0, 0, 1), P(0, 0, -1));
+    const V y2 = Ar::sub(S4(P(0, 1, 1), P(0, -1, 1), P(1, 0, 1), P(-1, 0, 1)),
+                         S4(P(0, 1, -1), P(0, -1, -1), P(1, 0, -1), P(-1, 0, -1)));
+    const V y3 = Ar::sub(S4(P(1, 1, 1), P(1, -1, 1), P(-1, 1, 1), P(-1, -1, 1)),
+                         S4(P(1, 1, -1), P(1, -1, -1), P(-1, 1, -1), P(-1, -1, -1)));
+    const V z1 = Ar::sub(P(1, 0, 0), P(-1, 0, 0));
+    const V z2 = Ar::sub(S4(P(1, 1, 0), P(1, -1, 0), P(1, 0, 1), P(1, 0, -1)),
+                         S4(P(-1, 1, 0), P(-1, -1, 0), P(-1, 0, 1), P(-1, 0, -1)));
+    const V z3 = Ar::sub(S4(P(1, 1, 1), P(1, 1, -1), P(1, -1, 1), P(1, -1, -1)),
+                         S4(P(-1, 1, 1), P(-1, 1, -1), P(-1, -1, 1), P(-1, -1, -1)));
+    const V c1 = Ar::c(3.f * wclass(1)), c2 = Ar::c(3.f * wclass(2)), c3 = Ar::c(3.f * wclass(3));
+    g[0] = Ar::fma(c3, x3, Ar::fma(c2, x2, Ar::mul(c1, x1)));
+    g[1] = Ar::fma(c3, y3, Ar::fma(c2, y2, Ar::mul(c1, y1)));
+    g[2] = Ar::fma(c3, z3, Ar::fma(c2, z2, Ar::mul(c1, z1)));
+}
+// one node; pm, p0, pp point at it in planes z-1, z, z+1 (row pitch SWv).
 // fp16 storage: the caller multiplies the result by the phi scale.
 template <int SWv, class T>
 __device__ __forceinline__ void grad_smem(const T* pm, const T* p0, const T* pp, float g[3]) {
-    auto P = [&](const T* pl, int dx, int dy) { return Stor<T>::ld(pl[dy * SWv + dx]); };
-    const float x1 = P(p0, 1, 0) - P(p0, -1, 0);
-    const float x2 = (P(p0, 1, 1) + P(p0, 1, -1) + P(pp, 1, 0) + P(pm, 1, 0)) -
-                     (P(p0, -1, 1) + P(p0, -1, -1) + P(pp, -1, 0) + P(pm, -1, 0));
-    const float x3 = (P(pp, 1, 1) + P(pp, 1, -1) + P(pm, 1, 1) + P(pm, 1, -1)) -
-                     (P(pp, -1, 1) + P(pp, -1, -1) + P(pm, -1, 1) + P(pm, -1, -1));
-    const float y1 = P(p0, 0, 1) - P(p0, 0, -1);
-    const float y2 = (P(p0, 1, 1) + P(p0, -1, 1) + P(pp, 0, 1) + P(pm, 0, 1)) -
-                     (P(p0, 1, -1) + P(p0, -1, -1) + P(pp, 0, -1) + P(pm, 0, -1));
-    const float y3 = (P(pp, 1, 1) + P(pp, -1, 1) + P(pm, 1, 1) + P(pm, -1, 1)) -
-                     (P(pp, 1, -1) + P(pp, -1, -1) + P(pm, 1, -1) + P(pm, -1, -1));
-    const float z1 = P(pp, 0, 0) - P(pm, 0, 0);
-    const float z2 = (P(pp, 1, 0) + P(pp, -1, 0) + P(pp, 0, 1) + P(pp, 0, -1)) -
-                     (P(pm, 1, 0) + P(pm, -1, 0) + P(pm, 0, 1) + P(pm, 0, -1));
-    const float z3 = (P(pp, 1, 1) + P(pp, 1, -1) + P(pp, -1, 1) + P(pp, -1, -1)) -
-                     (P(pm, 1, 1) + P(pm, 1, -1) + P(pm, -1, 1) + P(pm, -1, -1));
-    constexpr float c1 = 3.f * wclass(1), c2 = 3.f * wclass(2), c3 = 3.f * wclass(3);
-    g[0] = c1 * x1 + c2 * x2 + c3 * x3;
-    g[1] = c1 * y1 + c2 * y2 + c3 * y3;
-    g[2] = c1 * z1 + c2 * z2 + c3 * z3;
+    grad_v<Ar1>([&](int dz, int dx, int dy) {
+        const T* pl = dz < 0 ? pm : dz > 0 ? pp : p0;
+        return Stor<T>::ld(pl[dy * SWv + dx]);
+    }, g);
 }
 
 // Phase-field interface normal n = g / (|g| + 1e-9) from the staged phi
 // planes (ring slots of plane z and its neighbours), at staged offset pi
 // (recursive_2c_TSLB3D.f90:555-571).
+// n = g / (|g| + 1e-9) of one node (Ar1) or two (Ar2), operation by operation
+template <class Ar>
+__device__ __forceinline__ void normalize_v(typename Ar::V n[3]) {
+    const typename Ar::V m2 = Ar::fma(n[2], n[2], Ar::fma(n[1], n[1], Ar::mul(n[0], n[0])));
+    const typename Ar::V inv = Ar::map(m2, [](float x) { return __frcp_rn(__fadd_rn(sqrtf(x), 1e-9f)); });
+    n[0] = Ar::mul(n[0], inv); n[1] = Ar::mul(n[1], inv); n[2] = Ar::mul(n[2], inv);
+}
+// the phase field's interface indicator phi (1 - phi) |n|^2 (recursive_2c_TSLB3D.f90:614)
+template <class Ar>
+__device__ __forceinline__ typename Ar::V pf_indicator(typename Ar::V phi, const typename Ar::V n[3]) {
+    const typename Ar::V nn = Ar::fma(n[2], n[2], Ar::fma(n[1], n[1], Ar::mul(n[0], n[0])));
+    return Ar::mul(Ar::mul(phi, Ar::sub(Ar::c(1.f), phi)), nn);
+}
+
 template <int SWv, class T>
 __device__ __forceinline__ void pf_normal(const T* ring, int parea, int z, int pi, const StepArgs& a, float n[3]) {
     const T* p0 = ring + (z & (PRING - 1)) * parea + pi;
@@ -461,10 +485,10 @@ __device__ __forceinline__ void pf_normal(const T* ring, int parea, int z, int p
     const T* pp = ring + ((z + 1) & (PRING - 1)) * parea + pi;
     grad_smem<SWv>(pm, p0, pp, n);
     if constexpr (std::is_same<T, __half>::value) {
-        n[0] *= a.iscale[F_PHI]; n[1] *= a.iscale[F_PHI]; n[2] *= a.iscale[F_PHI];
+        n[0] = __fmul_rn(n[0], a.iscale[F_PHI]); n[1] = __fmul_rn(n[1], a.iscale[F_PHI]);
+        n[2] = __fmul_rn(n[2], a.iscale[F_PHI]);
     }
-    const float inv = __frcp_rn(sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) + 1e-9f);
-    n[0] *= inv; n[1] *= inv; n[2] *= inv;
+    normalize_v<Ar1>(n);
 }
 
 
@@ -530,7 +554,10 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // x faces and planes are staged with 16-byte cp.async copies.
 // One block's work: tile (bx, by) of columns and z chunk bz of lattice a.
 // SOLID: the lattice has interior solid nodes (bit masks a.solid, a.near).
-template <int MODE, bool VEC, class T, bool TAU = false, bool SOLID = false>
+// PAIR: the warps holding rim nodes compute their two coefficient nodes at
+// once (coef_pair); the results are the same numbers either way, so a form
+// whose registers are short (the phase field inside an ensemble) leaves it.
+template <int MODE, bool VEC, class T, bool TAU = false, bool SOLID = false, bool PAIR = true>
 __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, int bz) {
     constexpr int PHR = phi_halo(MODE);
     constexpr bool PHI = MODE != TSLB_MODE_SINGLE;   // phi is staged (colour, phase field)
@@ -771,7 +798,8 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                     m[F_PHI] = cvt_in<T>(*p0, a, F_PHI);
                     grad_smem<SW>(pm, p0, pp, g);
                     if constexpr (std::is_same<T, __half>::value) {
-                        g[0] *= a.iscale[F_PHI]; g[1] *= a.iscale[F_PHI]; g[2] *= a.iscale[F_PHI];
+                        g[0] = __fmul_rn(g[0], a.iscale[F_PHI]); g[1] = __fmul_rn(g[1], a.iscale[F_PHI]);
+                        g[2] = __fmul_rn(g[2], a.iscale[F_PHI]);
                     }
                 } else {
                     m[F_PHI] = 1.f;
@@ -779,6 +807,54 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 node_coefs<MODE, TAU>(a, m, g, 0.f, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs<MODE>(coef, ci, K);
+        };
+        // The warps that hold rim nodes (rows 0-2 of the tile: threads tid < NHALO)
+        // have two coefficient nodes per plane and set the length of the phase
+        // before the plane barrier.  They evaluate both at once on the paired
+        // FP32 instructions: lane x the own node, lane y the rim node (a thread
+        // without one repeats its own node in y and stores x alone).  Every
+        // operation rounds as in coef_node, so a node gets the same coefficients
+        // as an own node of one tile and as a rim node of another.
+        auto coef_pair = [&]() {
+            const XYNode nb = has_rim ? cn1 : cn0;
+            const int miB = has_rim ? mi1 : mi0, piB = has_rim ? pi1 : pi0;
+            Ar2::V m[NF], g[3] = {Ar2::c(0.f), Ar2::c(0.f), Ar2::c(0.f)};
+#pragma unroll
+            for (int f = 0; f < NMOM; ++f)
+                m[f] = make_float2(cvt_in<T>(ms[f * MAREA + mi0], a, f), cvt_in<T>(ms[f * MAREA + miB], a, f));
+            if (MODE == TSLB_MODE_COLOUR) {
+                const T* r0 = phis + (s & (PRING - 1)) * PAREA;
+                const T* rm = phis + ((s - 1) & (PRING - 1)) * PAREA;
+                const T* rp = phis + ((s + 1) & (PRING - 1)) * PAREA;
+                m[F_PHI] = make_float2(cvt_in<T>(r0[pi0], a, F_PHI), cvt_in<T>(r0[piB], a, F_PHI));
+                grad_v<Ar2>([&](int dz, int dx, int dy) {
+                    const T* pl = dz < 0 ? rm : dz > 0 ? rp : r0;
+                    const int o = dy * SW + dx;
+                    return make_float2(Stor<T>::ld(pl[pi0 + o]), Stor<T>::ld(pl[piB + o]));
+                }, g);
+                if constexpr (std::is_same<T, __half>::value) {
+                    const Ar2::V sc = Ar2::c(a.iscale[F_PHI]);
+                    g[0] = Ar2::mul(g[0], sc); g[1] = Ar2::mul(g[1], sc); g[2] = Ar2::mul(g[2], sc);
+                }
+            } else {
+                m[F_PHI] = Ar2::c(1.f);
+            }
+            const long long pz = (long long)gz * plane;
+            const Ar2::V dt = TAU ? make_float2(__ldg(a.dtau + pz + cn0.off), __ldg(a.dtau + pz + nb.off)) : Ar2::c(0.f);
+            Ar2::V K2[NCOEF];
+            node_coefs_v<MODE, TAU, Ar2>(a, m, g, Ar2::c(0.f), dt, K2);
+            // solid nodes (behind a face, or interior solids) send nothing
+            const bool s0 = cn0.out || (SOLID && bit_at(a.solid, pz + cn0.off));
+            const bool s1 = nb.out || (SOLID && bit_at(a.solid, pz + nb.off));
+            float K[NCOEF];
+#pragma unroll
+            for (int c = 0; c < NCOEF; ++c) K[c] = s0 ? 0.f : K2[c].x;
+            store_coefs<MODE>(coef, ci0, K);
+            if (has_rim) {
+#pragma unroll
+                for (int c = 0; c < NCOEF; ++c) K[c] = s1 ? 0.f : K2[c].y;
+                store_coefs<MODE>(coef, ci1, K);
+            }
         };
         // Phase field: the interface normal n = grad phi / (|grad phi| + 1e-9) of
         // the node (recursive_2c_TSLB3D.f90:555-571) and, where the indicator
@@ -796,12 +872,55 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
                 const float phi = cvt_in<T>(phis[(s & (PRING - 1)) * PAREA + pi], a, F_PHI);
                 m[F_PHI] = phi;
                 pf_normal<SW>(phis, PAREA, s, pi, a, g);
-                const bool need = phi * (1.f - phi) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 0.2f;
+                const bool need = pf_indicator<Ar1>(phi, g) > 0.2f;
                 // a node that needs the curvature was listed as a candidate (slot >= 0)
                 const float curv = need && slot >= 0 ? cq_curv[slot] : 0.f;
                 node_coefs<MODE, TAU>(a, m, g, curv, K, TAU ? (long long)gz * plane + nd.off : 0);
             }
             store_coefs<MODE>(coef, ci, K);
+        };
+        // the same two nodes at once for the phase field (coef_node_pf per lane)
+        auto coef_pair_pf = [&]() {
+            const XYNode nb = has_rim ? cn1 : cn0;
+            const int miB = has_rim ? mi1 : mi0, piB = has_rim ? pi1 : pi0, slotB = has_rim ? slot1 : slot0;
+            Ar2::V m[NF], g[3];
+#pragma unroll
+            for (int f = 0; f < NMOM; ++f)
+                m[f] = make_float2(cvt_in<T>(ms[f * MAREA + mi0], a, f), cvt_in<T>(ms[f * MAREA + miB], a, f));
+            const T* r0 = phis + (s & (PRING - 1)) * PAREA;
+            const T* rm = phis + ((s - 1) & (PRING - 1)) * PAREA;
+            const T* rp = phis + ((s + 1) & (PRING - 1)) * PAREA;
+            const Ar2::V phi = make_float2(cvt_in<T>(r0[pi0], a, F_PHI), cvt_in<T>(r0[piB], a, F_PHI));
+            m[F_PHI] = phi;
+            grad_v<Ar2>([&](int dz, int dx, int dy) {
+                const T* pl = dz < 0 ? rm : dz > 0 ? rp : r0;
+                const int o = dy * SW + dx;
+                return make_float2(Stor<T>::ld(pl[pi0 + o]), Stor<T>::ld(pl[piB + o]));
+            }, g);
+            if constexpr (std::is_same<T, __half>::value) {
+                const Ar2::V sc = Ar2::c(a.iscale[F_PHI]);
+                g[0] = Ar2::mul(g[0], sc); g[1] = Ar2::mul(g[1], sc); g[2] = Ar2::mul(g[2], sc);
+            }
+            normalize_v<Ar2>(g);
+            const Ar2::V ind = pf_indicator<Ar2>(phi, g);
+            // a node that needs the curvature was listed as a candidate (slot >= 0)
+            const Ar2::V curv = make_float2(ind.x > 0.2f && slot0 >= 0 ? cq_curv[slot0] : 0.f,
+                                            ind.y > 0.2f && slotB >= 0 ? cq_curv[slotB] : 0.f);
+            const long long pz = (long long)gz * plane;
+            const Ar2::V dt = TAU ? make_float2(__ldg(a.dtau + pz + cn0.off), __ldg(a.dtau + pz + nb.off)) : Ar2::c(0.f);
+            Ar2::V K2[NCOEF];
+            node_coefs_v<MODE, TAU, Ar2>(a, m, g, curv, dt, K2);
+            const bool s0 = cn0.out || (SOLID && bit_at(a.solid, pz + cn0.off));
+            const bool s1 = nb.out || (SOLID && bit_at(a.solid, pz + nb.off));
+            float K[NCOEF];
+#pragma unroll
+            for (int c = 0; c < NCOEF; ++c) K[c] = s0 ? 0.f : K2[c].x;
+            store_coefs<MODE>(coef, ci0, K);
+            if (has_rim) {
+#pragma unroll
+                for (int c = 0; c < NCOEF; ++c) K[c] = s1 ? 0.f : K2[c].y;
+                store_coefs<MODE>(coef, ci1, K);
+            }
         };
         if (MODE == TSLB_MODE_PHASEFIELD) {
             // curvatures of this plane's candidates, warp w taking entries w, w + 8, ...
@@ -823,11 +942,17 @@ __device__ __forceinline__ void step_block(const StepArgs& a, int bx, int by, in
         }
         if (!zsolid) {
             if constexpr (MODE == TSLB_MODE_PHASEFIELD) {
-                coef_node_pf(cn0, ci0, mi0, pi0, slot0);
-                if (has_rim) coef_node_pf(cn1, ci1, mi1, pi1, slot1);
+                if (PAIR && ty * TX < NHALO) {
+                    coef_pair_pf();
+                } else {
+                    coef_node_pf(cn0, ci0, mi0, pi0, slot0);
+                    if (!PAIR && has_rim) coef_node_pf(cn1, ci1, mi1, pi1, slot1);
+                }
+            } else if (PAIR && ty * TX < NHALO) {
+                coef_pair();
             } else {
                 coef_node(cn0, ci0, mi0, pi0);
-                if (has_rim) coef_node(cn1, ci1, mi1, pi1);
+                if (!PAIR && has_rim) coef_node(cn1, ci1, mi1, pi1);
             }
         }
         // phase field: candidates of the next source plane (its phi is staged)
@@ -963,7 +1088,7 @@ __global__ void __launch_bounds__(NTHR, 2) ensemble_kernel(const StepArgs* __res
             __syncthreads();
             cur = w.dom;
         }
-        step_block<MODE, VEC, T>(sa, w.bx, w.by, w.bz);
+        step_block<MODE, VEC, T, false, false, MODE != TSLB_MODE_PHASEFIELD>(sa, w.bx, w.by, w.bz);
         __syncthreads();
         // every thread has read `next` (it was read before this item's barriers)
         if (step) {

@@ -378,3 +378,42 @@ def test_one_column_between_walls():
     o64, _ = run_oracle(p, f, 60, fp64=True)
     o32, _ = run_oracle(p, f, 60, fp64=False)
     assert_parity_grouped(gpu, o64, o32, "one column")
+
+
+@pytest.mark.parametrize("mode", ["colour", "phasefield", "single"])
+def test_periodic_shift_is_bit_exact(mode):
+    """Translation invariance, bit for bit: on a fully periodic lattice,
+    stepping a state shifted by (5, 3, 2) nodes gives the shifted result of
+    stepping the state itself.  The shift moves every node to another place
+    in the 32 x 8 tiles of the step: own nodes of a tile become rim nodes of
+    its neighbours and rows move between the warps that compute the rim and
+    those that do not, so this holds only if a node's coefficients are the
+    same numbers wherever the step computes them."""
+    nx, ny, nz = 64, 24, 16
+    m = {"colour": capi.MODE_COLOUR, "phasefield": capi.MODE_PHASEFIELD, "single": capi.MODE_SINGLE}[mode]
+    if m == capi.MODE_SINGLE:
+        p = capi.make_params(mode=m, tau_a=0.6, force=[1e-5, 0.0, 0.0])
+    elif m == capi.MODE_PHASEFIELD:
+        p = capi.make_params(mode=m, tau_a=0.7, tau_b=0.7, sigma=0.01, sharp_c=0.9)
+    else:
+        p = capi.make_params(mode=m, tau_a=0.7, tau_b=0.9, sigma=0.01, beta=0.7, grad_threshold=1e-3,
+                             force=[1e-5, 0.0, 0.0])
+    rng = np.random.default_rng(11)
+    f = workloads.empty_fields(nx, ny, nz)
+    for k in ("u", "v", "w"):
+        f[k][:] = rng.normal(0, 0.02, f[k].shape)
+    for k in ("pxx", "pxy", "pxz", "pyy", "pyz", "pzz"):
+        f[k][:] = rng.normal(0, 1e-4, f[k].shape)
+    f["rho"][:] = 1.0 + rng.normal(0, 1e-3, f["rho"].shape)
+    if m != capi.MODE_SINGLE:
+        z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        r = np.sqrt((x - 20.3) ** 2 + (y - 9.6) ** 2 + (z - 7.2) ** 2)
+        t = np.tanh((6.0 - r) / 2.0)
+        f["phi"][:] = 0.5 * (1.0 + t) if m == capi.MODE_PHASEFIELD else t
+    shift, axes = (2, 3, 5), (0, 1, 2)   # (z, y, x) of the (nz, ny, nx) arrays
+    a, _ = run_gpu(p, f, 12)
+    b, _ = run_gpu(p, {k: np.roll(v, shift, axes) for k, v in f.items()}, 12)
+    for k in capi.FIELDS:
+        ra = np.roll(np.asarray(a[k]), shift, axes)
+        nbad = int(np.count_nonzero(ra != np.asarray(b[k])))
+        assert nbad == 0, f"{mode}: field {k} differs at {nbad} nodes after the shift"
