@@ -1959,8 +1959,10 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
         cudaError_t ce = cudaMemcpy(step_backup, e->d_step, sizeof(step_backup), cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) { release(); return efail(e, TSLB_ERR_CUDA, std::string("tune backup: ") + cudaGetErrorString(ce)); }
     }
+    // the persistent kernel: two or one resident blocks per SM taking the work
+    // items as they finish (one block per item, grid 0, is a tslb_ensemble_set_launch choice)
     const int zcands[] = {8, 16, 32, 64, 128, 1 << 20};
-    const int gcands[] = {kStepBlocksPerSM * e->sms, 0};
+    const int gcands[] = {kStepBlocksPerSM * e->sms, e->sms};
     float best = 1e30f;
     int bz = e->zchunk, bg = e->grid;
     cudaEvent_t t0, t1;
@@ -1974,7 +1976,7 @@ int tslb_ensemble_tune(tslb_ensemble* e, int* zchunk_out, int* grid_out) {
             e->grid = gr;
             rc = ens_build(e);
             if (rc) break;
-            const int reps = 4;
+            const int reps = 10;
             rc = ens_launch(e);  // warm-up
             cudaEventRecord(t0, e->stream);
             for (int r = 0; r < reps && rc == TSLB_OK; ++r) rc = ens_launch(e);

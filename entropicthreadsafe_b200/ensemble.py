@@ -2,7 +2,8 @@
 
 `Ensemble` wraps tslb_ensemble_*: members of different sizes advanced by
 one kernel launch per step (optionally K steps from a CUDA graph), with a
-timing autotuner for the z chunk and the grid.  `couette_droplets` draws
+timing autotuner for the z chunk and the resident grid of the persistent
+kernel.  `couette_droplets` draws
 the droplet-in-Couette domains of config 4 from a seed, and `deformation`
 measures the Taylor deformation D = (L - B)/(L + B) of a droplet.
 """
@@ -82,7 +83,8 @@ class Ensemble:
 
     def tune_results(self) -> list:
         """The last tune()'s timings: dicts of zchunk (1 << 20: whole
-        lattices), grid (0: one block per work item) and ms per step."""
+        lattices), grid (resident blocks of the persistent kernel) and ms
+        per step."""
         n = ctypes.c_int()
         self._check(self.L.tslb_ensemble_tune_results(self.h, 0, ctypes.byref(n), None, None, None))
         zc = (ctypes.c_int * max(n.value, 1))()

@@ -350,10 +350,11 @@ int  tslb_ensemble_download_moments(tslb_ensemble* e, int i,
                                     float* pxx, float* pxy, float* pxz,
                                     float* pyy, float* pyz, float* pzz, float* phi);
 int  tslb_ensemble_reduce(tslb_ensemble* e, int i, double out[TSLB_NREDUCE]);
-/* Autotuner: time the candidate z chunks and grid sizes on the uploaded
- * state (restored afterwards) and keep the fastest; returns the choice.
- * grid 0 is one block per work item; grid > 0 that many resident blocks
- * taking the items in list order (longest first) as they finish. */
+/* Autotuner of the persistent kernel: time 10 steps of each candidate z
+ * chunk with each resident grid (two and one blocks per SM, taking the work
+ * items in list order, longest first, as they finish) on the uploaded state
+ * (restored afterwards) and keep the fastest; returns the choice.  One block
+ * per work item (grid 0) is set only by tslb_ensemble_set_launch. */
 int  tslb_ensemble_tune(tslb_ensemble* e, int* zchunk, int* grid);
 /* The last tuning's timings, in the order they ran: *count rows (at most
  * max written) of z chunk (1 << 20: whole lattices), grid and milliseconds

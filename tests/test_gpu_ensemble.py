@@ -24,10 +24,11 @@ def test_ensemble_equals_single_runs_with_graph_and_tuner():
         for i, d in enumerate(doms):
             ens.upload_moments(i, d["fields"])
         zc, gr = ens.tune()
-        assert zc > 0
-        # the tuner's table: 6 z chunks x 2 grids, the choice is the fastest row
+        # the persistent kernel: a resident grid
+        assert zc > 0 and gr > 0
+        # the tuner's table: 6 z chunks x 2 resident grids, the choice is the fastest row
         rows = ens.tune_results()
-        assert len(rows) == 12 and all(r["ms"] > 0 for r in rows)
+        assert len(rows) == 12 and all(r["ms"] > 0 and r["grid"] > 0 for r in rows)
         best = min(rows, key=lambda r: r["ms"])
         assert (best["zchunk"], best["grid"]) == (zc, gr)
         ens.step(3)                 # plain launches (odd count)
