@@ -18,6 +18,9 @@ evaluation equals the serial loop):
   jet walls, inlet and boundary_cds_3D_module.f90:885-1050 (bcs_2c_turbulent_jet:
   outlet               bounce-back of the solid planes, regularized inlet at
                        k = 1, zero-gradient outlet at k = nz)
+  single component     TSLB_2C-mpi/lb_kernels_module.f90:21-206 (moments_TSLB),
+                       :423-566 (fused_TSLB_1c) and :583-730 (fused_TSLB_force_1c),
+                       stepped as TSLB_2C-mpi/recursive_TSbcs_TSLB3.f90:285-353 does
 
 Translation is mechanical: array references `a(i+1,j,k-1,q)` become
 shifted numpy views, `x_db` literals drop the kind suffix, `if` blocks
@@ -68,6 +71,11 @@ BLOCKS = {
     "bounceback": ("boundary_cds_3D_module.f90", 18, 70),
     "couette": ("boundary_cds_3D_module.f90", 413, 571),
     "jet": ("boundary_cds_3D_module.f90", 885, 1050),
+    # the single-component program (TSLB_2C-mpi/recursive_TSbcs_TSLB3.f90:285,346): moments_TSLB
+    # and fused_TSLB_1c, and the module's forced collision fused_TSLB_force_1c
+    "sc_moments": ("TSLB_2C-mpi/lb_kernels_module.f90", 21, 206),
+    "sc_collision": ("TSLB_2C-mpi/lb_kernels_module.f90", 423, 566),
+    "sc_collision_force": ("TSLB_2C-mpi/lb_kernels_module.f90", 583, 730),
 }
 
 
@@ -281,7 +289,47 @@ CASES = {
     "pf_droplet32": dict(n=(32, 32, 32), walls=None, collision="collision", nsteps=100,
                          tau=0.8, sigma=0.01, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.0,
                          droplet=(16.5, 16.5, 16.5, 8.0), urand=0.002, seed=15, moments_only=True),
+    # single component, fully periodic, from initial moments (random rho, u and Pi^neq)
+    # (relaxation times that FP32 holds exactly, as the C-ABI's parameters are FP32)
+    "sc_periodic": dict(n=(8, 6, 8), walls=None, single="sc_collision", nsteps=12, tau=0.6875,
+                        force=(0.0, 0.0, 0.0), urand=0.02, pirand=1e-4, seed=16),
+    "sc_force": dict(n=(8, 6, 8), walls=None, single="sc_collision_force", nsteps=12, tau=0.8125,
+                     force=(2.0 ** -14, 2.0 ** -16, 0.0), urand=0.02, pirand=1e-4, seed=17),
 }
+# the moments of a single-component state (no phi)
+SC_MOMENTS = MOMENTS[:-1]
+
+
+def run_case_single(ref: str, cfg: dict, dtype):
+    """The single-component program from a moment state: each step is the
+    collision-and-push block, the periodic population exchange, and
+    moments_TSLB (recursive_TSbcs_TSLB3.f90:285-353 in that order, entered
+    after its moments pass).  The initial moments are FP32 numbers, the same
+    for both precisions."""
+    nx, ny, nz = cfg["n"]
+    G = Grid(nx, ny, nz, dtype, (True, True, True))
+    rng = np.random.default_rng(cfg["seed"])
+    ic = {"rho": (1.0 + 1e-3 * rng.uniform(-1, 1, (nx, ny, nz))).astype(np.float32)}
+    for name in ("u", "v", "w"):
+        ic[name] = (cfg["urand"] * rng.uniform(-1, 1, (nx, ny, nz))).astype(np.float32)
+    for name in ("pxx", "pxy", "pxz", "pyy", "pyz", "pzz"):
+        ic[name] = (cfg["pirand"] * rng.uniform(-1, 1, (nx, ny, nz))).astype(np.float32)
+    for name in SC_MOMENTS:
+        G.a[name][1:-1, 1:-1, 1:-1] = ic[name].astype(dtype)
+    t = dtype
+    consts = {
+        "p0": t(8.0) / t(27.0), "p1": t(2.0) / t(27.0), "p2": t(1.0) / t(54.0), "p3": t(1.0) / t(216.0),
+        "omega": t(1.0) / t(cfg["tau"]),
+        "fx": t(cfg["force"][0]), "fy": t(cfg["force"][1]), "fz": t(cfg["force"][2]),
+    }
+    moments = parse(read_block(ref, *BLOCKS["sc_moments"]))
+    collision = parse(read_block(ref, *BLOCKS[cfg["single"]]))
+    for _ in range(cfg["nsteps"]):
+        G.run(collision, consts)
+        G.wrap_pops()
+        G.run(moments, consts)
+    out = {name: G.a[name][1:nx + 1, 1:ny + 1, 1:nz + 1].copy() for name in SC_MOMENTS}
+    return out, ic
 
 
 def run_case(ref: str, cfg: dict, dtype):
@@ -328,7 +376,7 @@ def run_case(ref: str, cfg: dict, dtype):
         "fx": t(cfg["force"][0]), "fy": t(cfg["force"][1]), "fz": t(cfg["force"][2]),
         "uwall": t(cfg["uwall"]),
     }
-    tree = {name: parse(read_block(ref, *BLOCKS[name])) for name in BLOCKS}
+    tree = {name: parse(read_block(ref, *BLOCKS[name])) for name in BLOCKS if not name.startswith("sc_")}
     # the one rewritten index: `nz-1` of the jet block occurs in its k == nz branch only
     jet_text = " ".join(read_block(ref, *BLOCKS["jet"])).replace(" ", "")
     assert jet_text.count("nz-1") == 1 and jet_text.index("elseif(k.eq.nz)") < jet_text.index("nz-1")
@@ -400,6 +448,24 @@ def main():
     for name, cfg in CASES.items():
         if args.case and name not in args.case:
             continue
+        if cfg.get("single"):
+            res = {}
+            outs = {}
+            for tag, dt in (("fp64", np.float64), ("fp32", np.float32)):
+                out, ic = run_case_single(args.reference, cfg, dt)
+                outs[tag] = out
+                for m in SC_MOMENTS:
+                    res[f"{m}_{tag}"] = to_oracle_layout(out[m])
+            for m in SC_MOMENTS:
+                res[f"ic_{m}"] = to_oracle_layout(ic[m])
+            meta = dict(cfg)
+            meta["blocks"] = {k: list(BLOCKS[k]) for k in ("sc_moments", cfg["single"])}
+            res["meta"] = np.array(json.dumps(meta))
+            path = os.path.join(args.out, f"{name}.npz")
+            np.savez_compressed(path, **res)
+            d = max(np.abs(outs["fp32"][m] - outs["fp64"][m]).max() for m in SC_MOMENTS)
+            print(f"{name}: wrote {path} ({os.path.getsize(path)} B); max |fp32-fp64| = {d:.3e}")
+            continue
         res = {}
         outs = {}
         for tag, dt in (("fp64", np.float64), ("fp32", np.float32)):
@@ -427,7 +493,7 @@ def main():
         if inlet is not None:
             res["inlet"] = np.ascontiguousarray(np.swapaxes(inlet, -1, -2))   # (4, ny, nx): u, v, w, phi of the z- face
         meta = dict(cfg)
-        meta["blocks"] = {k: list(v) for k, v in BLOCKS.items()}
+        meta["blocks"] = {k: list(v) for k, v in BLOCKS.items() if not k.startswith("sc_")}
         res["meta"] = np.array(json.dumps(meta))
         path = os.path.join(args.out, f"{name}.npz")
         np.savez_compressed(path, **res)

@@ -6,7 +6,10 @@ the phase-field step recursive_2c_TSLB3D.f90:351-832, the forced collision
 TSLB_2C-mpi/lb_kernels_module.f90:747-931, bounce-back
 boundary_cds_3D_module.f90:18-70, the moving-wall condition
 boundary_cds_3D_module.f90:413-571 and the jet's inlet and outlet
-boundary_cds_3D_module.f90:885-1050 (with a fixed inlet plane).
+boundary_cds_3D_module.f90:885-1050 (with a fixed inlet plane); and the
+single-component program's moments_TSLB, fused_TSLB_1c and
+fused_TSLB_force_1c (TSLB_2C-mpi/lb_kernels_module.f90:21-206, 423-566,
+583-730), stepped from a moment state.
 """
 import json
 
@@ -80,3 +83,43 @@ def test_oracle_fp64_matches_reference_statements_32cube_100_steps():
         assert rel_err(a, b) < 1e-6, m
     spread = json.loads(str(d["fp32_spread"]))
     assert set(spread) == set(capi.FIELDS)
+
+
+# the single-component program's own statements (moments_TSLB, fused_TSLB_1c,
+# fused_TSLB_force_1c of TSLB_2C-mpi/lb_kernels_module.f90)
+SC_CASES = ("sc_periodic", "sc_force")
+SC_FIELDS = tuple(f for f in capi.FIELDS if f != "phi")
+
+
+@pytest.mark.parametrize("fp64", [True, False], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("case", SC_CASES)
+def test_single_component_oracle_matches_reference_statements(case, fp64):
+    """TSLB_MODE_SINGLE of the oracle (the phase-field step at sigma = 0 with
+    a uniform phi, as the GPU single-component kernel is checked against)
+    from the fixture's initial moments, against the reference's
+    single-component statements over the same steps: unforced (sc_periodic)
+    and with the forced collision's velocity shift (sc_force)."""
+    d, meta = load(case)
+    ic = {k: d["ic_" + k].astype(np.float64) for k in SC_FIELDS}
+    nz, ny, nx = ic["rho"].shape
+    ic["phi"] = np.ones((nz, ny, nx))
+    p = capi.make_params(mode=capi.MODE_SINGLE, tau_a=meta["tau"], sigma=0.0, force=meta["force"])
+    o = oracle.Oracle(p, nx, ny, nz, fp64=fp64)
+    o.set_moments(ic)
+    o.step(meta["nsteps"])
+    out = o.get_moments()
+    o.close()
+    tag = "fp64" if fp64 else "fp32"
+    for m in SC_FIELDS:
+        a, b = out[m], d[m + "_" + tag].astype(np.float64)
+        if m == "rho":
+            a, b = a - 1.0, b - 1.0
+        if fp64:
+            # double-precision round-off of two algebraically equal forms (the
+            # non-equilibrium moments are sums of O(1) populations of size 1e-4)
+            assert rel_err(a, b) < 1e-11, (m, rel_err(a, b))
+        else:
+            # FP32 round-off relative to each field's max (rho - 1 and Pi^neq of
+            # size 1e-3 and 1e-4): the reference's own FP32 statements differ
+            # from their FP64 run by up to 4e-4
+            assert rel_err(a, b) < 1e-3, (m, rel_err(a, b))
