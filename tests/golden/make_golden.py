@@ -13,7 +13,8 @@ evaluation equals the serial loop):
   normals pass         recursive_2c_TSLB3D.f90:547-574
   collision + push     recursive_2c_TSLB3D.f90:612-832
   collision with force TSLB_2C-mpi/lb_kernels_module.f90:747-931
-  bounce-back          boundary_cds_3D_module.f90:18-70
+  bounce-back          boundary_cds_3D_module.f90:18-70 (at wall planes, and at
+                       the nodes of an interior obstacle)
   moving walls         boundary_cds_3D_module.f90:413-571
   jet walls, inlet and boundary_cds_3D_module.f90:885-1050 (bcs_2c_turbulent_jet:
   outlet               bounce-back of the solid planes, regularized inlet at
@@ -289,6 +290,11 @@ CASES = {
     "pf_droplet32": dict(n=(32, 32, 32), walls=None, collision="collision", nsteps=100,
                          tau=0.8, sigma=0.01, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.0,
                          droplet=(16.5, 16.5, 16.5, 8.0), urand=0.002, seed=15, moments_only=True),
+    # fully periodic droplet beside an interior obstacle (isfluid = 0 nodes, i, j, k ranges
+    # inclusive, 1-based): the bounce-back block acts at every solid node
+    "pf_obstacle": dict(n=(8, 8, 8), walls=None, collision="collision", nsteps=12,
+                        tau=0.75, sigma=0.01, sharp_c=0.9, force=(0.0, 0.0, 0.0), uwall=0.0,
+                        droplet=(3.5, 4.5, 4.5, 2.0), urand=0.01, seed=18, obstacle=(5, 6, 3, 5, 3, 6)),
     # single component, fully periodic, from initial moments (random rho, u and Pi^neq)
     # (relaxation times that FP32 holds exactly, as the C-ABI's parameters are FP32)
     "sc_periodic": dict(n=(8, 6, 8), walls=None, single="sc_collision", nsteps=12, tau=0.6875,
@@ -340,6 +346,9 @@ def run_case(ref: str, cfg: dict, dtype):
     if walls:
         G.a["isfluid"][:, :, 1] = 0
         G.a["isfluid"][:, :, nz] = 0
+    if cfg.get("obstacle"):
+        i0, i1, j0, j1, k0, k1 = cfg["obstacle"]
+        G.a["isfluid"][i0:i1 + 1, j0:j1 + 1, k0:k1 + 1] = 0
     rng = np.random.default_rng(cfg["seed"])
     i, j, k = np.meshgrid(np.arange(1, nx + 1), np.arange(1, ny + 1), np.arange(1, nz + 1), indexing="ij")
     fluid = G.a["isfluid"][1:-1, 1:-1, 1:-1] == 1
@@ -415,7 +424,7 @@ def run_case(ref: str, cfg: dict, dtype):
             G.wrap_scalar(name)
         run_block(cfg["collision"])
         G.wrap_pops()
-        if walls == "bounceback":
+        if walls == "bounceback" or cfg.get("obstacle"):
             run_block("bounceback")
         elif walls == "couette":
             for name in MOMENTS:
